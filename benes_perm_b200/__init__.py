@@ -1,0 +1,257 @@
+# SPDX-License-Identifier: Apache-2.0
+"""B200 compression backend for benes-perm: Python host mirror.
+
+Mirrors the reference's public compression API (include/benes/benes.hpp:
+``FormatOptions``, ``CompressOptions``, ``compress``, ``backend_available``,
+``backend_name``) for the one backend this package provides.  Every call goes
+through the C ABI in ``include/benes_b200.h`` into ``libbenes_b200.so``; there
+is no CPU fallback.  Errors raise the Python counterparts of the reference's
+exception types: ``ValueError`` for std::invalid_argument, ``OverflowError``
+for std::overflow_error, ``MemoryError``-free ``LengthError`` for
+std::length_error and ``RuntimeError`` for std::runtime_error.
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "libbenes_b200.so")
+
+
+class LengthError(ValueError):
+    """std::length_error counterpart."""
+
+
+class MiddlePlacement(enum.IntEnum):
+    """benes::MiddlePlacement (include/benes/benes.hpp:21-25)."""
+
+    separate = 0
+    embedded_input = 1
+    embedded_output = 2
+
+
+class InputValueWidth(enum.IntEnum):
+    """benes::InputValueWidth (include/benes/benes.hpp:27-30)."""
+
+    bits32 = 4
+    bits64 = 8
+
+
+class PermutationKind(enum.IntEnum):
+    """Synthetic permutation generators (workload inputs)."""
+
+    uniform = 0       # Fisher-Yates
+    single_cycle = 1  # Sattolo
+    identity = 2
+    reverse = 3
+    bit_reversal = 4
+
+
+@dataclass
+class FormatOptions:
+    """benes::FormatOptions (include/benes/benes.hpp:32-39)."""
+
+    middle_group_log2: int = 5
+    input_clusters: Sequence[int] = field(default_factory=list)
+    output_clusters: Sequence[int] = field(default_factory=list)
+    middle_placement: MiddlePlacement = MiddlePlacement.separate
+
+
+@dataclass
+class CompressOptions:
+    """benes::CompressOptions (include/benes/benes.hpp:41-45); ``threads`` is
+    accepted and ignored, like the reference's GPU backends."""
+
+    threads: int = 0
+    format: FormatOptions = field(default_factory=FormatOptions)
+
+
+class _Format(ctypes.Structure):
+    _fields_ = [
+        ("middle_group_log2", ctypes.c_uint8),
+        ("middle_placement", ctypes.c_uint8),
+        ("input_cluster_count", ctypes.c_uint8),
+        ("output_cluster_count", ctypes.c_uint8),
+        ("input_clusters", ctypes.c_uint8 * 64),
+        ("output_clusters", ctypes.c_uint8 * 64),
+    ]
+
+
+def to_c_format(fmt: Optional[FormatOptions]) -> _Format:
+    fmt = fmt or FormatOptions()
+    if len(fmt.input_clusters) > 64 or len(fmt.output_clusters) > 64:
+        raise ValueError("cluster depths do not span every routing level")
+    c = _Format()
+    c.middle_group_log2 = int(fmt.middle_group_log2) & 0xFF
+    c.middle_placement = int(fmt.middle_placement) & 0xFF
+    c.input_cluster_count = len(fmt.input_clusters)
+    c.output_cluster_count = len(fmt.output_clusters)
+    for i, v in enumerate(fmt.input_clusters):
+        c.input_clusters[i] = int(v) & 0xFF
+    for i, v in enumerate(fmt.output_clusters):
+        c.output_clusters[i] = int(v) & 0xFF
+    return c
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Loads libbenes_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIBRARY_PATH):
+            raise ImportError(
+                f"{LIBRARY_PATH} is missing: build it with `python benes_perm_b200/build.py`"
+            )
+        lib = ctypes.CDLL(LIBRARY_PATH)
+        u8p = ctypes.POINTER(ctypes.c_uint8)
+        fp = ctypes.POINTER(_Format)
+        lib.bpb200_available.restype = ctypes.c_int
+        lib.bpb200_backend_name.restype = ctypes.c_char_p
+        lib.bpb200_encoded_size.argtypes = [ctypes.c_uint64, fp, ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.c_char_p, ctypes.c_size_t]
+        lib.bpb200_compress.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, fp,
+                                        u8p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.c_char_p, ctypes.c_size_t]
+        lib.bpb200_compress_device.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32,
+                                               fp, ctypes.c_void_p, ctypes.c_uint64,
+                                               ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                               ctypes.c_char_p, ctypes.c_size_t]
+        lib.bpb200_fill_permutation.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                                ctypes.c_uint32, ctypes.c_void_p]
+        lib.bpb200_probe_switch_bit.argtypes = [ctypes.c_uint64, fp, ctypes.c_int, ctypes.c_uint32,
+                                                ctypes.c_uint64, ctypes.c_uint64,
+                                                ctypes.POINTER(ctypes.c_uint64)]
+        lib.bpb200_probe_rank_bit.argtypes = [ctypes.c_uint64, fp, ctypes.c_uint32, ctypes.c_uint64,
+                                              ctypes.POINTER(ctypes.c_int),
+                                              ctypes.POINTER(ctypes.c_uint64)]
+        lib.bpb200_shutdown.restype = None
+        _lib = lib
+    return _lib
+
+
+def raise_for(code: int, message: str) -> None:
+    if code == 0:
+        return
+    if code == 1:
+        raise ValueError(message)
+    if code == 2:
+        raise OverflowError(message)
+    if code == 3:
+        raise LengthError(message)
+    raise RuntimeError(message or f"b200 backend error {code}")
+
+
+def backend_available() -> bool:
+    """backend_available(Backend::b200)."""
+    try:
+        return bool(library().bpb200_available())
+    except OSError:
+        return False
+
+
+def backend_name() -> str:
+    return library().bpb200_backend_name().decode()
+
+
+def encoded_size(count: int, fmt: Optional[FormatOptions] = None) -> int:
+    err = ctypes.create_string_buffer(256)
+    out = ctypes.c_uint64(0)
+    cf = to_c_format(fmt)
+    raise_for(library().bpb200_encoded_size(count, ctypes.byref(cf), ctypes.byref(out), err, 256),
+              err.value.decode())
+    return out.value
+
+
+_last_device_seconds = 0.0
+
+
+def last_device_seconds() -> float:
+    """detail::last_device_seconds() of the most recent compress call."""
+    return _last_device_seconds
+
+
+def compress(permutation, options: Optional[CompressOptions] = None) -> bytes:
+    """benes::compress(span<const uint32_t|uint64_t>, {.backend = b200, ...}).
+
+    ``permutation`` is a 1-D numpy array (or buffer-protocol object) of
+    uint32 or uint64 values.  Returns the canonical version-1 blob.
+    """
+    global _last_device_seconds
+    options = options or CompressOptions()
+    arr = np.ascontiguousarray(permutation)
+    if arr.dtype not in (np.uint32, np.uint64):
+        raise TypeError("permutation must be uint32 or uint64")
+    n = int(arr.size)
+    cf = to_c_format(options.format)
+    err = ctypes.create_string_buffer(512)
+    size = ctypes.c_uint64(0)
+    if n == 0:
+        raise ValueError("permutation size is out of range")
+    raise_for(library().bpb200_encoded_size(n, ctypes.byref(cf), ctypes.byref(size), err, 512),
+              err.value.decode())
+    blob = np.empty(size.value, dtype=np.uint8)
+    secs = ctypes.c_double(0)
+    rc = library().bpb200_compress(
+        arr.ctypes.data, n, arr.dtype.itemsize, ctypes.byref(cf),
+        blob.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), size.value,
+        ctypes.byref(secs), err, 512)
+    raise_for(rc, err.value.decode())
+    _last_device_seconds = secs.value
+    return blob.tobytes()
+
+
+def compress_device(d_entries: int, count: int, entry_bytes: int, d_blob: int, blob_len: int,
+                    fmt: Optional[FormatOptions] = None, stream: int = 0) -> float:
+    """Device-resident compress: device pointers in, device blob out.
+    Returns device seconds."""
+    cf = to_c_format(fmt)
+    err = ctypes.create_string_buffer(512)
+    secs = ctypes.c_double(0)
+    rc = library().bpb200_compress_device(d_entries, count, entry_bytes, ctypes.byref(cf),
+                                          d_blob, blob_len, stream, ctypes.byref(secs), err, 512)
+    raise_for(rc, err.value.decode())
+    return secs.value
+
+
+def fill_permutation(kind: PermutationKind, seed: int, count: int,
+                     dtype=np.uint32, out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Seeded synthetic permutation (xoshiro256** from splitmix64(seed))."""
+    dtype = np.dtype(dtype)
+    if out is None:
+        out = np.empty(count, dtype=dtype)
+    rc = library().bpb200_fill_permutation(int(kind), seed & 0xFFFFFFFFFFFFFFFF, count,
+                                           out.dtype.itemsize, out.ctypes.data)
+    raise_for(rc, "invalid permutation request")
+    return out
+
+
+def probe_switch_bit(count: int, fmt: FormatOptions, side: int, level: int, node: int,
+                     pair: int) -> int:
+    cf = to_c_format(fmt)
+    out = ctypes.c_uint64(0)
+    rc = library().bpb200_probe_switch_bit(count, ctypes.byref(cf), side, level, node, pair,
+                                           ctypes.byref(out))
+    raise_for(rc, "no such switch")
+    return out.value
+
+
+def probe_rank_bit(count: int, fmt: FormatOptions, level: int, node: int):
+    cf = to_c_format(fmt)
+    sec = ctypes.c_int(0)
+    out = ctypes.c_uint64(0)
+    rc = library().bpb200_probe_rank_bit(count, ctypes.byref(cf), level, node, ctypes.byref(sec),
+                                         ctypes.byref(out))
+    raise_for(rc, "not a leaf")
+    return sec.value, out.value
+
+
+def shutdown() -> None:
+    library().bpb200_shutdown()

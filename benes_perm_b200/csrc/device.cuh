@@ -1,0 +1,231 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// Device building blocks shared by the level kernels and the tile kernel:
+// parity union-find, warp-aggregated bit emission and the warp factoradic
+// rank.
+#pragma once
+
+#include "plan.hpp"
+
+#include <cstdint>
+
+namespace bpb200 {
+
+// Device status word bits (read by the host after each call).
+constexpr uint32_t kErrNotPermutation = 1u;  // value out of range or duplicated
+constexpr uint32_t kErrIterationCap = 2u;    // a bounded retry loop gave up
+constexpr uint32_t kErrInconsistent = 4u;    // colouring constraint violated
+
+// Retry bound for every lock-free loop; far above what a valid input needs.
+// Parents strictly decrease along every union-find chain (links go to the
+// smaller root, halving jumps to the grandparent), so loops end anyway; the
+// bound only caps the cost of a pathological chain.
+constexpr uint32_t kSpinCap = 1u << 20;
+
+// ------------------------------------------------------------------------
+// Parity union-find over pair-nodes.
+//
+// Word layout: (parent << 1) | bit.  For a non-root the bit is the colour
+// difference between the node and its parent; a root points to itself and
+// its bit is the orientation flag set after all unions (it flips the colour
+// of the whole component so that the odd tail ends up colour 0).  Linking
+// always hangs the larger root under the smaller, so a root is the smallest
+// pair-node of its component and parents strictly decrease along any chain.
+// Path halving stores (grandparent, accumulated bit); the colour difference
+// between a node and any ancestor is fixed by the constraint graph, so such
+// racy plain stores can only ever write true facts.
+// ------------------------------------------------------------------------
+
+struct Found {
+    uint32_t root;
+    uint32_t bit;
+};
+
+template <typename Word>
+__device__ __forceinline__ Word uf_load(Word* uf, uint32_t i) {
+    return *((volatile Word*)(uf + i));
+}
+
+template <typename Word>
+__device__ __forceinline__ Found uf_find(Word* uf, uint32_t x, uint32_t* err) {
+    uint32_t acc = 0;
+    uint32_t cur = x;
+    for (uint32_t it = 0; it < kSpinCap; ++it) {
+        const uint32_t w = (uint32_t)uf_load(uf, cur);
+        const uint32_t p = w >> 1;
+        if (p == cur) {
+            return {cur, acc};
+        }
+        const uint32_t wp = (uint32_t)uf_load(uf, p);
+        const uint32_t pp = wp >> 1;
+        if (pp == p) {
+            return {p, acc ^ (w & 1u)};
+        }
+        const uint32_t nb = (w ^ wp) & 1u;
+        uf[cur] = (Word)((pp << 1) | nb);
+        acc ^= nb;
+        cur = pp;
+    }
+    atomicOr(err, kErrIterationCap);
+    return {cur, acc};
+}
+
+__device__ __forceinline__ uint32_t cas_word(uint32_t* a, uint32_t e, uint32_t v) {
+    return atomicCAS(a, e, v);
+}
+
+// Record x(a) ^ x(b) == rel.
+template <typename Word>
+__device__ __forceinline__ void uf_union(Word* uf, uint32_t a, uint32_t b, uint32_t rel,
+    uint32_t* err) {
+    for (uint32_t it = 0; it < kSpinCap; ++it) {
+        const Found fa = uf_find(uf, a, err);
+        const Found fb = uf_find(uf, b, err);
+        rel ^= fa.bit ^ fb.bit;
+        a = fa.root;
+        b = fb.root;
+        if (a == b) {
+            if (rel != 0) {
+                atomicOr(err, kErrInconsistent);
+            }
+            return;
+        }
+        const uint32_t lo = a < b ? a : b;
+        const uint32_t hi = a < b ? b : a;
+        if (cas_word((uint32_t*)(uf + hi), hi << 1, (lo << 1) | rel) == (hi << 1)) {
+            return;
+        }
+    }
+    atomicOr(err, kErrIterationCap);
+}
+
+// ------------------------------------------------------------------------
+// Warp-aggregated emission of single bits into the blob.  Lanes of the
+// warp named in `active` call it together; each lane with `set` ORs bit
+// `abs_bit` (absolute bit position in the blob).  Lanes that hit the same
+// 32-bit word combine first, so one atomic is issued per distinct word.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ void emit_bit(uint32_t* blob, uint64_t abs_bit, bool set,
+    unsigned active) {
+    const unsigned writers = __ballot_sync(active, set);
+    if (!set) {
+        return;
+    }
+    const unsigned long long word = abs_bit >> 5;
+    const unsigned group = __match_any_sync(writers, word);
+    const unsigned v = __reduce_or_sync(group, 1u << (abs_bit & 31));
+    if ((threadIdx.x & 31) == (unsigned)(__ffs(group) - 1)) {
+        atomicOr(blob + word, v);
+    }
+}
+
+// ------------------------------------------------------------------------
+// 128-bit helpers for the factoradic rank.
+// ------------------------------------------------------------------------
+struct U128 {
+    unsigned long long lo, hi;
+};
+
+__device__ __forceinline__ U128 mul128(U128 a, U128 b) {
+    U128 r;
+    r.lo = a.lo * b.lo;
+    r.hi = __umul64hi(a.lo, b.lo) + a.lo * b.hi + a.hi * b.lo;
+    return r;
+}
+
+__device__ __forceinline__ U128 add128(U128 a, U128 b) {
+    U128 r;
+    r.lo = a.lo + b.lo;
+    r.hi = a.hi + b.hi + (r.lo < a.lo ? 1ull : 0ull);
+    return r;
+}
+
+__device__ __forceinline__ U128 shfl_down128(U128 v, int d) {
+    U128 r;
+    r.lo = __shfl_down_sync(0xffffffffu, v.lo, d);
+    r.hi = __shfl_down_sync(0xffffffffu, v.hi, d);
+    return r;
+}
+
+// Factoradic rank of one middle group held one entry per lane (lanes
+// >= count are idle), as in encode_factoradic (src/internal.hpp:148-167):
+// digit j = #{k < j : v[k] < v[j]} and rank = sum_j digit_j * count!/(j+1)!.
+// Digits come from five ballots (a one-hot lane mask per value) and a
+// prefix-OR over values; the mixed-radix sum is an order-preserving tree
+// reduction of (rank, radix product) pairs: (r1,m1)+(r2,m2) = (r1*m2+r2, m1*m2).
+// Must be called by all 32 lanes.  Result valid in lane 0.  *distinct is
+// false (in every lane) when two lanes hold the same value.
+__device__ __forceinline__ U128 warp_factoradic_rank(uint32_t value, uint32_t count,
+    bool* distinct) {
+    const unsigned lane = threadIdx.x & 31;
+    const bool live = lane < count;
+    const unsigned active = __ballot_sync(0xffffffffu, live);
+    unsigned onehot = active;
+    for (int b = 0; b < 5; ++b) {
+        const unsigned bits = __ballot_sync(0xffffffffu, live && ((value >> b) & 1));
+        onehot &= ((lane >> b) & 1) ? bits : ~bits;
+    }
+    // with count values below count, every value has exactly one lane iff
+    // no value is missing
+    *distinct = __ballot_sync(0xffffffffu, live && __popc(onehot) != 1) == 0;
+    // onehot (in lane L) = the lane holding value L.  Exclusive prefix OR
+    // over values gives the lanes holding a smaller value.
+    unsigned below = onehot;
+    for (int d = 1; d < 32; d <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, below, d);
+        if ((int)lane >= d) {
+            below |= t;
+        }
+    }
+    below = __shfl_up_sync(0xffffffffu, below, 1);
+    if (lane == 0) {
+        below = 0;
+    }
+    const unsigned smaller = __shfl_sync(0xffffffffu, below, live ? value : 0);
+    const uint32_t digit = live ? (uint32_t)__popc(smaller & ((1u << lane) - 1u)) : 0u;
+    U128 r = {digit, 0ull};
+    U128 m = {live ? (unsigned long long)(lane + 1) : 1ull, 0ull};
+    for (int d = 1; d < 32; d <<= 1) {
+        const U128 r2 = shfl_down128(r, d);
+        const U128 m2 = shfl_down128(m, d);
+        if ((lane & (2 * d - 1)) == 0) {
+            r = add128(mul128(r, m2), r2);
+            m = mul128(m, m2);
+        }
+    }
+    return r;
+}
+
+// OR `nbits` (<= 118) bits of `rank` into the blob at absolute bit `abs`.
+// Lanes 0..4 each handle one destination word.  All lanes call.
+__device__ __forceinline__ void emit_rank(uint32_t* blob, uint64_t abs, uint32_t nbits,
+    U128 rank) {
+    const unsigned lane = threadIdx.x & 31;
+    rank.lo = __shfl_sync(0xffffffffu, rank.lo, 0);
+    rank.hi = __shfl_sync(0xffffffffu, rank.hi, 0);
+    if (nbits == 0 || lane >= 5) {
+        return;
+    }
+    const uint32_t shift = (uint32_t)(abs & 31);
+    const uint64_t word0 = abs >> 5;
+    const uint32_t last = (uint32_t)((shift + nbits - 1) >> 5);
+    if (lane > last) {
+        return;
+    }
+    // bits of the rank that land in destination word `lane`
+    const int lo_bit = (int)lane * 32 - (int)shift; // rank bit at dest bit 0 of this word
+    uint32_t v = 0;
+    for (int b = 0; b < 32; ++b) {
+        const int rb = lo_bit + b;
+        if (rb < 0 || rb >= (int)nbits) {
+            continue;
+        }
+        const unsigned long long src = rb < 64 ? rank.lo : rank.hi;
+        v |= (uint32_t)((src >> (rb & 63)) & 1ull) << b;
+    }
+    if (v != 0) {
+        atomicOr(blob + word0 + lane, v);
+    }
+}
+
+} // namespace bpb200

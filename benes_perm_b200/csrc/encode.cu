@@ -1,0 +1,572 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// Host orchestration and C ABI of the B200 compact encoder.
+//
+// One call: plan on the host (closed-form layout, a few KB) -> prologue
+// kernel (zero status, header bytes) -> level kernels for the levels whose
+// nodes exceed a tile -> one tile kernel finishing every subtree in shared
+// memory.  Everything runs on one stream; scratch lives in a pooled
+// per-device workspace so repeated calls allocate nothing.
+#include "../../include/benes_b200.h"
+#include "kernels.cuh"
+#include "layout.hpp"
+#include "plan.hpp"
+#include "tile.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace bpb200 {
+namespace {
+
+constexpr uint64_t kTileMaxEntries = 8192;
+constexpr uint32_t kTileSmemBudget = 200 * 1024;
+constexpr int kLevelThreads = 256;
+
+struct CudaFail {
+    cudaError_t err;
+    const char* what;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) {
+        throw CudaFail{e, what};
+    }
+}
+
+// ------------------------------------------------------------ workspace
+
+struct Workspace {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    Plan* d_plan = nullptr;
+    Plan* h_plan = nullptr;       // pinned staging for the plan upload
+    uint32_t* d_status = nullptr;
+    uint32_t* h_status = nullptr; // pinned
+    uint32_t* vals[2] = {nullptr, nullptr};
+    uint32_t* inv = nullptr;
+    uint32_t* uf = nullptr;
+    uint32_t* xbits = nullptr;
+    NodeAddress* addr[2] = {nullptr, nullptr};
+    uint64_t slot_cap = 0, pair_cap = 0, node_cap = 0;
+    void* input = nullptr;        // staging for host-path inputs
+    uint64_t input_cap = 0;
+    uint32_t* blob = nullptr;     // staging for host-path blobs
+    uint64_t blob_cap = 0;
+    bool busy = false;
+
+    void release_scratch() {
+        for (void* p : {(void*)vals[0], (void*)vals[1], (void*)inv, (void*)uf, (void*)xbits,
+                 (void*)addr[0], (void*)addr[1]}) {
+            if (p) cudaFree(p);
+        }
+        vals[0] = vals[1] = inv = uf = xbits = nullptr;
+        addr[0] = addr[1] = nullptr;
+        slot_cap = pair_cap = node_cap = 0;
+    }
+    void destroy() {
+        release_scratch();
+        if (input) cudaFree(input);
+        if (blob) cudaFree(blob);
+        if (d_plan) cudaFree(d_plan);
+        if (d_status) cudaFree(d_status);
+        if (h_plan) cudaFreeHost(h_plan);
+        if (h_status) cudaFreeHost(h_status);
+        if (start) cudaEventDestroy(start);
+        if (stop) cudaEventDestroy(stop);
+        if (stream) cudaStreamDestroy(stream);
+        *this = Workspace();
+    }
+};
+
+std::mutex g_pool_mutex;
+std::vector<std::unique_ptr<Workspace>> g_pool;
+
+Workspace* acquire(int device) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    for (auto& w : g_pool) {
+        if (!w->busy && w->device == device) {
+            w->busy = true;
+            return w.get();
+        }
+    }
+    auto w = std::make_unique<Workspace>();
+    w->device = device;
+    check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreate(&w->start), "cudaEventCreate");
+    check(cudaEventCreate(&w->stop), "cudaEventCreate");
+    check(cudaMalloc(&w->d_plan, sizeof(Plan)), "cudaMalloc(plan)");
+    check(cudaMallocHost(&w->h_plan, sizeof(Plan)), "cudaMallocHost(plan)");
+    check(cudaMalloc(&w->d_status, sizeof(uint32_t)), "cudaMalloc(status)");
+    check(cudaMallocHost(&w->h_status, sizeof(uint32_t)), "cudaMallocHost(status)");
+    w->busy = true;
+    g_pool.push_back(std::move(w));
+    return g_pool.back().get();
+}
+
+void release(Workspace* w) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    w->busy = false;
+}
+
+struct Lease {
+    Workspace* w;
+    explicit Lease(int device) : w(acquire(device)) {}
+    ~Lease() { release(w); }
+};
+
+void ensure_scratch(Workspace& w, const Plan& p) {
+    const uint64_t slots = p.tile_level > 0 ? p.max_slots : 0;
+    const uint64_t pairs = p.tile_level > 0 ? p.max_pairs : 0;
+    const uint64_t nodes = p.tile_level > 0 ? (1ull << (p.tile_level - 1)) : 0;
+    if (slots <= w.slot_cap && pairs <= w.pair_cap && nodes <= w.node_cap) {
+        return;
+    }
+    w.release_scratch();
+    if (slots == 0) {
+        return;
+    }
+    check(cudaMalloc(&w.vals[0], slots * 4), "cudaMalloc(level array)");
+    check(cudaMalloc(&w.vals[1], slots * 4), "cudaMalloc(level array)");
+    check(cudaMalloc(&w.inv, slots * 4), "cudaMalloc(inverse)");
+    check(cudaMalloc(&w.uf, pairs * 4), "cudaMalloc(union-find)");
+    check(cudaMalloc(&w.xbits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(colour bits)");
+    check(cudaMalloc(&w.addr[0], nodes * sizeof(NodeAddress)), "cudaMalloc(descriptors)");
+    check(cudaMalloc(&w.addr[1], nodes * sizeof(NodeAddress)), "cudaMalloc(descriptors)");
+    w.slot_cap = slots;
+    w.pair_cap = pairs;
+    w.node_cap = nodes;
+}
+
+// ------------------------------------------------------------ prologue
+
+struct Header {
+    uint32_t bytes;
+    uint8_t data[84];
+};
+
+__global__ void prologue(uint32_t* status, uint32_t* blob, Header h) {
+    if (threadIdx.x == 0) {
+        *status = 0;
+    }
+    // the header ends before the first section bit; only whole header bytes
+    // are written, so it cannot clobber section bits sharing its last word
+    uint8_t* b = reinterpret_cast<uint8_t*>(blob);
+    for (uint32_t i = threadIdx.x; i < h.bytes; i += blockDim.x) {
+        b[i] = h.data[i];
+    }
+}
+
+// ------------------------------------------------------------ tile sizing
+
+TileShape tile_shape(const Plan& p, uint32_t t0) {
+    uint64_t slots = 0, pairs = 0;
+    for (uint32_t l = t0; l <= p.depth; ++l) {
+        const uint64_t n = 1ull << (l - t0);
+        slots = std::max<uint64_t>(slots, n * p.levels[l].cap);
+        pairs = std::max<uint64_t>(pairs, n * p.levels[l].pcap);
+    }
+    TileShape s;
+    s.slots = (uint32_t)std::min<uint64_t>(slots, 1u << 30);
+    s.pairs = (uint32_t)std::min<uint64_t>(pairs, 1u << 30);
+    uint32_t off[7];
+    s.smem = tile_smem_layout(s.slots, s.pairs, off);
+    if (slots >= 65536 || pairs >= (1u << 30)) {
+        s.smem = UINT32_MAX;
+    }
+    return s;
+}
+
+// Picks the tile level: the first level whose nodes fit a tile whose
+// deepest padded level also fits the shared-memory budget.
+void choose_tile(Plan& p, TileShape* shape) {
+    uint32_t t0 = 0;
+    while (t0 < p.depth && p.levels[t0].cap > kTileMaxEntries) {
+        ++t0;
+    }
+    TileShape s = tile_shape(p, t0);
+    while (s.smem > kTileSmemBudget && t0 < p.depth) {
+        ++t0;
+        s = tile_shape(p, t0);
+    }
+    p.tile_level = t0;
+    uint64_t slots = 0, pairs = 0;
+    for (uint32_t l = 0; l <= t0; ++l) {
+        slots = std::max<uint64_t>(slots, (1ull << l) * p.levels[l].cap);
+        pairs = std::max<uint64_t>(pairs, (1ull << l) * p.levels[l].pcap);
+    }
+    p.max_slots = slots;
+    p.max_pairs = pairs;
+    *shape = s;
+}
+
+int grid_for(uint64_t work, int threads) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = (work + threads - 1) / threads;
+    const uint64_t cap = (uint64_t)sms * 16;
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(want, cap));
+}
+
+template <typename T>
+void launch_levels(Workspace& w, const Plan& p, const TileShape& shape, const T* d_in,
+    uint32_t* d_blob) {
+    cudaStream_t st = w.stream;
+    const Plan* dp = w.d_plan;
+    const uint32_t t0 = p.tile_level;
+    if (t0 > 0) {
+        // level 0 validation: inverse slots start as 0xffffffff so a
+        // duplicated value leaves a never-written slot behind
+        check(cudaMemsetAsync(w.inv, 0xff, p.levels[0].cap * 4, st), "cudaMemsetAsync");
+    }
+    const uint32_t* cur32 = nullptr;
+    for (uint32_t l = 0; l < t0; ++l) {
+        const LevelInfo& lv = p.levels[l];
+        const uint64_t slots = lv.cap << l;
+        const uint64_t prs = lv.pcap << l;
+        const uint64_t nodes = 1ull << l;
+        uint32_t* dst = w.vals[l & 1];
+        const int gs = grid_for(slots, kLevelThreads);
+        const int gp = grid_for(prs, kLevelThreads);
+        const int gn = grid_for(nodes, kLevelThreads);
+        if (l == 0) {
+            level_inverse<T><<<gs, kLevelThreads, 0, st>>>(dp, l, d_in, w.inv, w.uf, w.d_status);
+        } else {
+            level_inverse<uint32_t><<<gs, kLevelThreads, 0, st>>>(dp, l, cur32, w.inv, w.uf,
+                w.d_status);
+        }
+        level_descriptors<<<gn, kLevelThreads, 0, st>>>(dp, l, w.addr[0], w.addr[1]);
+        level_union<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
+        level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
+        if (l == 0) {
+            level_resolve<T><<<gp, kLevelThreads, 0, st>>>(dp, l, d_in, w.uf, w.xbits, dst,
+                w.addr[0], d_blob, w.d_status);
+        } else {
+            level_resolve<uint32_t><<<gp, kLevelThreads, 0, st>>>(dp, l, cur32, w.uf, w.xbits,
+                dst, w.addr[0], d_blob, w.d_status);
+        }
+        level_output_bits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.addr[1], d_blob);
+        check(cudaGetLastError(), "level kernel launch");
+        cur32 = dst;
+    }
+    const uint64_t tiles = 1ull << t0;
+    if (tiles > 0x7fffffffull) {
+        throw CudaFail{cudaErrorInvalidValue, "too many tiles"};
+    }
+    if (t0 == 0) {
+        check(cudaFuncSetAttribute(tile_encode<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                  (int)shape.smem), "cudaFuncSetAttribute");
+        tile_encode<T><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, d_in, d_blob,
+            w.d_status, shape.slots, shape.pairs);
+    } else {
+        check(cudaFuncSetAttribute(tile_encode<uint32_t>,
+                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape.smem),
+            "cudaFuncSetAttribute");
+        tile_encode<uint32_t><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, cur32,
+            d_blob, w.d_status, shape.slots, shape.pairs);
+    }
+    check(cudaGetLastError(), "tile kernel launch");
+}
+
+struct Call {
+    Layout layout;
+    Plan* plan = nullptr;
+    TileShape shape{};
+};
+
+void set_error(char* err, size_t len, const std::string& msg) {
+    if (err != nullptr && len > 0) {
+        std::snprintf(err, len, "%s", msg.c_str());
+    }
+}
+
+Format to_format(const bpb200_format* f) {
+    Format out;
+    if (f == nullptr) {
+        return out;
+    }
+    out.middle_group_log2 = f->middle_group_log2;
+    out.middle_placement = f->middle_placement;
+    out.input_cluster_count = f->input_cluster_count;
+    out.output_cluster_count = f->output_cluster_count;
+    std::memcpy(out.input_clusters, f->input_clusters, 64);
+    std::memcpy(out.output_clusters, f->output_clusters, 64);
+    return out;
+}
+
+// Validation shared by both entry points; fills the layout and plan.
+int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
+    uint64_t blob_len, Workspace& w, Call* call, char* err, size_t err_len) {
+    if (entry_bytes != 4 && entry_bytes != 8) {
+        set_error(err, err_len, "entry width must be 4 or 8 bytes");
+        return kInvalidArgument;
+    }
+    if (count == 0) {
+        set_error(err, err_len, "permutation size is out of range");
+        return kInvalidArgument;
+    }
+    if (entry_bytes == 4 && count > 0xffffffffull) {
+        set_error(err, err_len, "permutation size requires 64-bit source values");
+        return kInvalidArgument;
+    }
+    Error e = make_layout(count, to_format(format), &call->layout);
+    if (!e.ok()) {
+        set_error(err, err_len, e.message);
+        return e.code;
+    }
+    if (count > (1ull << 31)) {
+        set_error(err, err_len, "the b200 backend handles at most 2^31 entries");
+        return kLength;
+    }
+    if (blob_len != call->layout.end_offset) {
+        set_error(err, err_len, "blob length does not match the encoded size");
+        return kLength;
+    }
+    call->plan = w.h_plan;
+    e = make_plan(call->layout, kTileMaxEntries, call->plan);
+    if (!e.ok()) {
+        set_error(err, err_len, e.message);
+        return e.code;
+    }
+    choose_tile(*call->plan, &call->shape);
+    if (call->shape.smem > kTileSmemBudget) {
+        set_error(err, err_len, "tile does not fit in shared memory");
+        return kLength;
+    }
+    return kOk;
+}
+
+// Queues the whole encode on w.stream and waits for it.
+int run(Workspace& w, Call& call, const void* d_in, uint32_t entry_bytes, uint32_t* d_blob,
+    double* device_seconds, char* err, size_t err_len) {
+    const Plan& p = *call.plan;
+    ensure_scratch(w, p);
+    cudaStream_t st = w.stream;
+    check(cudaMemcpyAsync(w.d_plan, w.h_plan, sizeof(Plan), cudaMemcpyHostToDevice, st),
+        "plan upload");
+    Header h{};
+    h.bytes = (uint32_t)call.layout.header_bytes;
+    write_header(call.layout, h.data);
+    check(cudaEventRecord(w.start, st), "cudaEventRecord");
+    check(cudaMemsetAsync(d_blob, 0, (p.end_offset + 3) / 4 * 4, st), "cudaMemsetAsync(blob)");
+    prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h);
+    if (entry_bytes == 4) {
+        launch_levels<uint32_t>(w, p, call.shape, (const uint32_t*)d_in, d_blob);
+    } else {
+        launch_levels<uint64_t>(w, p, call.shape, (const uint64_t*)d_in, d_blob);
+    }
+    check(cudaEventRecord(w.stop, st), "cudaEventRecord");
+    check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
+    check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, w.start, w.stop), "cudaEventElapsedTime");
+    if (device_seconds) {
+        *device_seconds = ms * 1e-3;
+    }
+    const uint32_t status = *w.h_status;
+    if (status & kErrNotPermutation) {
+        set_error(err, err_len, "input must contain every value from zero through size minus one");
+        return kInvalidArgument;
+    }
+    if (status & (kErrIterationCap | kErrInconsistent)) {
+        set_error(err, err_len, "b200 device status reported a failed colouring");
+        return kRuntime;
+    }
+    return kOk;
+}
+
+int current_device_ok(int* device) {
+    if (cudaGetDevice(device) != cudaSuccess) {
+        return 0;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, *device) != cudaSuccess) {
+        return 0;
+    }
+    return prop.major == 10 ? 1 : 0;
+}
+
+template <typename Fn>
+int guarded(char* err, size_t err_len, Fn&& fn) {
+    try {
+        return fn();
+    } catch (const CudaFail& f) {
+        set_error(err, err_len, std::string(f.what) + ": " + cudaGetErrorString(f.err));
+        return kRuntime;
+    } catch (const std::bad_alloc&) {
+        set_error(err, err_len, "host allocation failed");
+        return kRuntime;
+    }
+}
+
+} // namespace
+} // namespace bpb200
+
+using namespace bpb200;
+
+extern "C" {
+
+int bpb200_available(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        return 0;
+    }
+    int device = 0;
+    return current_device_ok(&device);
+}
+
+const char* bpb200_backend_name(void) { return "b200"; }
+
+int bpb200_encoded_size(uint64_t count, const bpb200_format* format, uint64_t* blob_bytes,
+    char* err, size_t err_len) {
+    Layout L;
+    const Error e = make_layout(count, to_format(format), &L);
+    if (!e.ok()) {
+        set_error(err, err_len, e.message);
+        return e.code;
+    }
+    *blob_bytes = L.end_offset;
+    return kOk;
+}
+
+int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* blob, uint64_t blob_len, double* device_seconds,
+    char* err, size_t err_len) {
+    return guarded(err, err_len, [&]() -> int {
+        int device = 0;
+        if (!current_device_ok(&device)) {
+            set_error(err, err_len, "b200 backend is unavailable");
+            return kUnavailable;
+        }
+        Lease lease(device);
+        Workspace& w = *lease.w;
+        Call call;
+        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+        if (rc != kOk) {
+            return rc;
+        }
+        const uint64_t in_bytes = count * entry_bytes;
+        if (in_bytes > w.input_cap) {
+            if (w.input) cudaFree(w.input);
+            w.input = nullptr;
+            w.input_cap = 0;
+            check(cudaMalloc(&w.input, in_bytes), "cudaMalloc(input)");
+            w.input_cap = in_bytes;
+        }
+        const uint64_t blob_words = (blob_len + 3) / 4 + 1;
+        if (blob_words * 4 > w.blob_cap) {
+            if (w.blob) cudaFree(w.blob);
+            w.blob = nullptr;
+            w.blob_cap = 0;
+            check(cudaMalloc(&w.blob, blob_words * 4), "cudaMalloc(blob)");
+            w.blob_cap = blob_words * 4;
+        }
+        check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
+            "input upload");
+        rc = run(w, call, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
+        if (rc != kOk) {
+            return rc;
+        }
+        check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
+            "blob download");
+        check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
+        return kOk;
+    });
+}
+
+int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, void* stream,
+    double* device_seconds, char* err, size_t err_len) {
+    return guarded(err, err_len, [&]() -> int {
+        int device = 0;
+        if (!current_device_ok(&device)) {
+            set_error(err, err_len, "b200 backend is unavailable");
+            return kUnavailable;
+        }
+        if (((uintptr_t)d_blob & 3u) != 0) {
+            set_error(err, err_len, "device blob must be 4-byte aligned");
+            return kInvalidArgument;
+        }
+        Lease lease(device);
+        Workspace& w = *lease.w;
+        Call call;
+        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+        if (rc != kOk) {
+            return rc;
+        }
+        cudaStream_t user = (cudaStream_t)stream;
+        // order the workspace stream after the caller's prior work, and the
+        // caller's later work after ours
+        cudaEvent_t ev;
+        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+        check(cudaEventRecord(ev, user), "cudaEventRecord");
+        check(cudaStreamWaitEvent(w.stream, ev, 0), "cudaStreamWaitEvent");
+        rc = run(w, call, d_entries, entry_bytes, (uint32_t*)d_blob, device_seconds, err, err_len);
+        cudaEventDestroy(ev);
+        return rc;
+    });
+}
+
+void bpb200_shutdown(void) {
+    std::lock_guard<std::mutex> lock(g_pool_mutex);
+    for (auto& w : g_pool) {
+        if (!w->busy) {
+            w->destroy();
+        }
+    }
+    g_pool.erase(std::remove_if(g_pool.begin(), g_pool.end(),
+                     [](const std::unique_ptr<Workspace>& w) { return w->device < 0; }),
+        g_pool.end());
+}
+
+int bpb200_probe_switch_bit(uint64_t count, const bpb200_format* format, int side,
+    uint32_t level, uint64_t node, uint64_t pair, uint64_t* bit) {
+    Layout L;
+    if (!make_layout(count, to_format(format), &L).ok()) {
+        return kInvalidArgument;
+    }
+    std::unique_ptr<Plan> p(new Plan);
+    if (!make_plan(L, kTileMaxEntries, p.get()).ok()) {
+        return kInvalidArgument;
+    }
+    if (level >= L.depth || node >= (1ull << level) || (side != 0 && side != 1)) {
+        return kInvalidArgument;
+    }
+    const uint64_t size = node_size(p->levels[level], level, node);
+    if (size <= p->leaf || pair >= size / 2) {
+        return kInvalidArgument;
+    }
+    *bit = switch_bit(node_address(*p, side, level, node), pair);
+    return kOk;
+}
+
+int bpb200_probe_rank_bit(uint64_t count, const bpb200_format* format, uint32_t level,
+    uint64_t node, int* section, uint64_t* bit) {
+    Layout L;
+    if (!make_layout(count, to_format(format), &L).ok()) {
+        return kInvalidArgument;
+    }
+    std::unique_ptr<Plan> p(new Plan);
+    if (!make_plan(L, kTileMaxEntries, p.get()).ok()) {
+        return kInvalidArgument;
+    }
+    if (level > L.depth || node >= (1ull << level)) {
+        return kInvalidArgument;
+    }
+    if (node_size(p->levels[level], level, node) > p->leaf) {
+        return kInvalidArgument;
+    }
+    *bit = leaf_rank_bit(*p, level, node, section);
+    return kOk;
+}
+
+} // extern "C"

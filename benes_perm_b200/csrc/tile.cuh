@@ -1,0 +1,282 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// Tile kernel: one CTA per node of the tile level; the node's whole subtree
+// (every remaining routing level plus the middle-group ranks) is encoded in
+// shared memory.  Node-local values fit 16 bits (a tile holds at most a few
+// thousand entries), union-find words are 32-bit smem words.
+#pragma once
+
+#include "device.cuh"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+#include <cstdint>
+
+namespace bpb200 {
+
+struct TileSmem {
+    uint16_t* vals[2];
+    uint16_t* inv;
+    uint32_t* uf;
+    uint32_t* xbits;
+    NodeAddress* desc;  // [2][kNodeWave]
+    uint64_t* leafbit;  // [kNodeWave], section in the top 2 bits
+};
+
+__host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
+
+// Byte offsets of the smem arrays; identical on host (sizing) and device.
+__host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pairs,
+    uint32_t* off) {
+    uint32_t o = 0;
+    off[0] = o; o = align_up(o + slots * 2, 16);           // vals[0]
+    off[1] = o; o = align_up(o + slots * 2, 16);           // vals[1]
+    off[2] = o; o = align_up(o + slots * 2, 16);           // inv
+    off[3] = o; o = align_up(o + pairs * 4, 16);           // uf
+    off[4] = o; o = align_up(o + (pairs + 31) / 32 * 4 + 4, 16); // xbits
+    off[5] = o; o = align_up(o + 2 * kNodeWave * (uint32_t)sizeof(NodeAddress), 16);
+    off[6] = o; o = align_up(o + kNodeWave * 8, 16);       // leafbit
+    return o;
+}
+
+__device__ __forceinline__ bool node_exists(const Plan& p, uint32_t level, uint64_t node) {
+    if (level == 0) {
+        return true;
+    }
+    return node_size(p.levels[level - 1], level - 1, node >> 1) > p.leaf;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restrict__ plan_ptr,
+    const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
+    uint32_t pairs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t off[7];
+    tile_smem_layout(slots, pairs, off);
+    uint16_t* vals[2] = {(uint16_t*)(smem + off[0]), (uint16_t*)(smem + off[1])};
+    uint16_t* inv = (uint16_t*)(smem + off[2]);
+    uint32_t* uf = (uint32_t*)(smem + off[3]);
+    uint32_t* xbits = (uint32_t*)(smem + off[4]);
+    NodeAddress* desc = (NodeAddress*)(smem + off[5]);
+    uint64_t* leafbit = (uint64_t*)(smem + off[6]);
+
+    const Plan& plan = *plan_ptr;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31;
+    const uint32_t warp = tid >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t T0 = plan.tile_level;
+    const uint32_t D = plan.depth;
+    const uint32_t leaf = plan.leaf;
+    const uint64_t J = blockIdx.x;
+
+    if (!node_exists(plan, T0, J)) {
+        return;
+    }
+    {
+        const LevelInfo& l0 = plan.levels[T0];
+        const uint32_t s0 = (uint32_t)node_size(l0, T0, J);
+        const T* in = src + J * l0.cap;
+        for (uint32_t i = tid; i < s0; i += blockDim.x) {
+            const uint64_t v = (uint64_t)in[i];
+            if (v >= s0) {
+                atomicOr(status, kErrNotPermutation);
+                vals[0][i] = 0;
+            } else {
+                vals[0][i] = (uint16_t)v;
+            }
+        }
+    }
+    __syncthreads();
+
+    for (uint32_t t = 0;; ++t) {
+        const uint32_t level = T0 + t;
+        const LevelInfo& lv = plan.levels[level];
+        const uint32_t cap = (uint32_t)lv.cap;
+        const uint32_t pcap = (uint32_t)lv.pcap;
+        const uint32_t nodes = 1u << t;
+        const uint64_t first = J << t;
+        uint16_t* cur = vals[t & 1];
+        uint16_t* nxt = vals[(t + 1) & 1];
+
+        if (level < D) {
+            if (t == 0 && T0 == 0) {
+                // the whole permutation is in this tile: mark inverse slots so
+                // duplicates show up as never-written entries
+                for (uint32_t e = tid; e < cap; e += blockDim.x) {
+                    inv[e] = 0xffffu;
+                }
+                __syncthreads();
+            }
+            // A: inverse and union-find init
+            for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
+                const uint32_t path = e / cap;
+                const uint32_t i = e - path * cap;
+                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                if (i >= s || s <= leaf || !node_exists(plan, level, first + path)) {
+                    continue;
+                }
+                const uint32_t v = cur[e];
+                if (v >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                    continue;
+                }
+                inv[path * cap + v] = (uint16_t)i;
+                if ((i & 1u) == 0) {
+                    const uint32_t id = path * pcap + (i >> 1);
+                    uf[id] = id << 1;
+                }
+            }
+            __syncthreads();
+            // B: one union per output pair
+            for (uint32_t p = tid; p < nodes * pcap; p += blockDim.x) {
+                const uint32_t path = p / pcap;
+                const uint32_t k = p - path * pcap;
+                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                if (s <= leaf || k >= s / 2 || !node_exists(plan, level, first + path)) {
+                    continue;
+                }
+                const uint32_t u = inv[path * cap + 2 * k];
+                const uint32_t w = inv[path * cap + 2 * k + 1];
+                if (u >= s || w >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                    continue;
+                }
+                const uint32_t base = path * pcap;
+                uf_union(uf, base + (u >> 1), base + (w >> 1), 1u ^ (u & 1u) ^ (w & 1u), status);
+            }
+            __syncthreads();
+            // C: orient odd nodes so the unpaired tail gets colour 0
+            for (uint32_t path = tid; path < nodes; path += blockDim.x) {
+                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                if (s <= leaf || (s & 1u) == 0 || !node_exists(plan, level, first + path)) {
+                    continue;
+                }
+                if (inv[path * cap + s - 1] >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                    continue;
+                }
+                const Found f = uf_find(uf, path * pcap + (s >> 1), status);
+                if (f.bit) {
+                    atomicOr(uf + f.root, 1u);
+                }
+            }
+            __syncthreads();
+            // D: colours, child scatter
+            const uint32_t ccap = (uint32_t)plan.levels[level + 1].cap;
+            const uint32_t ptotal = nodes * pcap;
+            for (uint32_t base = warp * 32; base < ptotal; base += nwarps * 32) {
+                const uint32_t p = base + lane;
+                uint32_t x = 0;
+                if (p < ptotal) {
+                    const uint32_t path = p / pcap;
+                    const uint32_t k = p - path * pcap;
+                    const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                    if (s > leaf && k < s - s / 2 && node_exists(plan, level, first + path)) {
+                        const Found f = uf_find(uf, p, status);
+                        x = f.bit ^ (uf_load(uf, f.root) & 1u);
+                        const uint32_t node = path * cap;
+                        const uint32_t half = s / 2;
+                        if (k < half) {
+                            nxt[2 * path * ccap + k] = (uint16_t)(cur[node + 2 * k + x] >> 1);
+                            nxt[(2 * path + 1) * ccap + k] = (uint16_t)(cur[node + 2 * k + 1 - x] >> 1);
+                        } else {
+                            nxt[2 * path * ccap + k] = (uint16_t)(cur[node + s - 1] >> 1);
+                        }
+                    }
+                }
+                const unsigned word = __ballot_sync(0xffffffffu, x != 0);
+                if (lane == 0) {
+                    xbits[base >> 5] = word;
+                }
+            }
+            __syncthreads();
+            // E: switch bits, a wave of node descriptors at a time
+            for (uint32_t w0 = 0; w0 < nodes; w0 += kNodeWave) {
+                const uint32_t wn = nodes - w0 < kNodeWave ? nodes - w0 : kNodeWave;
+                if (tid < 2 * kNodeWave) {
+                    const uint32_t slot = tid >> 1;
+                    const int side = (int)(tid & 1);
+                    if (slot < wn) {
+                        const uint64_t node = first + w0 + slot;
+                        if (node_size(lv, level, node) > leaf && node_exists(plan, level, node)) {
+                            desc[side * kNodeWave + slot] = node_address(plan, side, level, node);
+                        }
+                    }
+                }
+                __syncthreads();
+                const uint32_t p0 = w0 * pcap;
+                const uint32_t p1 = (w0 + wn) * pcap;
+                const uint64_t in_bit0 = plan.section_offset[0] * 8;
+                const uint64_t out_bit0 = plan.section_offset[1] * 8;
+                for (uint32_t base = p0 + warp * 32; base < p1; base += nwarps * 32) {
+                    const uint32_t p = base + lane;
+                    bool has = false, xin = false, yout = false;
+                    uint64_t ib = 0, ob = 0;
+                    if (p < p1) {
+                        const uint32_t path = p / pcap;
+                        const uint32_t k = p - path * pcap;
+                        const uint64_t node = first + path;
+                        const uint32_t s = (uint32_t)node_size(lv, level, node);
+                        if (s > leaf && k < s / 2 && node_exists(plan, level, node)) {
+                            has = true;
+                            xin = (xbits[p >> 5] >> (p & 31)) & 1u;
+                            const uint32_t u = inv[path * cap + 2 * k];
+                            const uint32_t q = path * pcap + (u >> 1);
+                            yout = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                            const uint32_t slot = path - w0;
+                            ib = in_bit0 + switch_bit(desc[slot], k);
+                            ob = out_bit0 + switch_bit(desc[kNodeWave + slot], k);
+                        }
+                    }
+                    emit_bit(blob, ib, has && xin, 0xffffffffu);
+                    emit_bit(blob, ob, has && yout, 0xffffffffu);
+                }
+                __syncthreads();
+            }
+        }
+
+        // leaves at this level (all of level D, and the size-`leaf` nodes of a
+        // mixed level D - 1)
+        if (lv.q <= leaf) {
+            for (uint32_t w0 = 0; w0 < nodes; w0 += kNodeWave) {
+                const uint32_t wn = nodes - w0 < kNodeWave ? nodes - w0 : kNodeWave;
+                if (tid < wn) {
+                    const uint64_t node = first + w0 + tid;
+                    uint64_t v = ~0ull;
+                    if (node_size(lv, level, node) <= leaf && node_exists(plan, level, node)) {
+                        int section = 0;
+                        const uint64_t bit = leaf_rank_bit(plan, level, node, &section);
+                        v = plan.section_offset[section] * 8 + bit;
+                    }
+                    leafbit[tid] = v;
+                }
+                __syncthreads();
+                for (uint32_t li = warp; li < wn; li += nwarps) {
+                    const uint64_t at = leafbit[li];
+                    if (at == ~0ull) {
+                        continue;
+                    }
+                    const uint32_t path = w0 + li;
+                    const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                    const uint32_t v = lane < s ? (uint32_t)cur[path * cap + lane] : 0u;
+                    if (lane < s && v >= s) {
+                        atomicOr(status, kErrNotPermutation);
+                    }
+                    bool distinct = true;
+                    const U128 rank = warp_factoradic_rank(v < s ? v : 0u, s, &distinct);
+                    if (!distinct && lane == 0) {
+                        atomicOr(status, kErrNotPermutation);
+                    }
+                    emit_rank(blob, at, plan.fact_bits[s], rank);
+                }
+                __syncthreads();
+            }
+        }
+        if (level >= D) {
+            break;
+        }
+    }
+}
+
+} // namespace bpb200

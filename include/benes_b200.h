@@ -1,0 +1,104 @@
+/* SPDX-License-Identifier: Apache-2.0
+ *
+ * C ABI of the B200 compression backend for benes-perm.
+ *
+ * Every entry point is plain C: pointers, sizes and status codes, no C++ or
+ * torch types.  The reference library binds these from a thin C++ shim that
+ * plugs in beside its other accelerated backends; the
+ * status codes map one-to-one onto the exception types the reference throws.
+ */
+#ifndef BENES_B200_H
+#define BENES_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  Reference exception each one becomes in the C++ shim. */
+#define BPB200_OK 0
+#define BPB200_INVALID_ARGUMENT 1 /* std::invalid_argument (bad input or format) */
+#define BPB200_OVERFLOW 2         /* std::overflow_error (checked size arithmetic) */
+#define BPB200_LENGTH 3           /* std::length_error (does not fit) */
+#define BPB200_RUNTIME 4          /* std::runtime_error (CUDA or device status) */
+#define BPB200_UNAVAILABLE 6      /* std::runtime_error("b200 backend is unavailable") */
+
+/* benes::FormatOptions (include/benes/benes.hpp:32-39).  A cluster count of
+ * zero selects the reference's balanced default (src/internal.hpp:328-338). */
+typedef struct bpb200_format {
+    uint8_t middle_group_log2;    /* 1..5; the reference default is 5 */
+    uint8_t middle_placement;     /* 0 separate, 1 embedded_input, 2 embedded_output */
+    uint8_t input_cluster_count;  /* entries used in input_clusters */
+    uint8_t output_cluster_count; /* entries used in output_clusters */
+    uint8_t input_clusters[64];
+    uint8_t output_clusters[64];
+} bpb200_format;
+
+/* Replaces detail::cuda_available() (src/internal.hpp:1190; stub pattern
+ * src/backends_stub.cpp:25-26): nonzero when a B200-class (sm_100) device is
+ * visible and the kernels of this library can run on it. */
+int bpb200_available(void);
+
+/* Replaces backend_name(Backend::cuda) (src/benes.cpp:772-780): "b200". */
+const char* bpb200_backend_name(void);
+
+/* make_layout(count, format).end_offset (src/internal.hpp:389-429): the
+ * exact blob size in bytes.  Same validation and error kinds as the
+ * reference (invalid format -> INVALID_ARGUMENT, overflow -> OVERFLOW). */
+int bpb200_encoded_size(uint64_t count, const bpb200_format* format,
+    uint64_t* blob_bytes, char* err, size_t err_len);
+
+/* Replaces detail::compress_compact_cuda(span<const uint32_t|uint64_t>,
+ * FormatOptions) (src/internal.hpp:1192-1197; src/cuda/benes_cuda.cu:1155,
+ * 1334).  `entries` is host memory holding `count` little-endian values of
+ * `entry_bytes` (4 or 8) bytes.  Writes exactly `blob_len` bytes (which must
+ * equal bpb200_encoded_size) into `blob`, byte-identical to the reference's
+ * portable encoder.  `device_seconds` (may be NULL) receives the on-device
+ * time, the value the reference stores with set_last_device_seconds.
+ * Errors: INVALID_ARGUMENT "input must contain every value from zero through
+ * size minus one" for a non-permutation, exactly like validate_permutation
+ * (src/benes.cpp:152-173). */
+int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* blob, uint64_t blob_len,
+    double* device_seconds, char* err, size_t err_len);
+
+/* Device-resident form of bpb200_compress (no reference counterpart; the
+ * reference copies host spans, src/cuda/benes_cuda.cu:1397-1409).
+ * `d_entries` and `d_blob` are device pointers on the current device;
+ * `d_blob` must be 4-byte aligned with room for blob_len rounded up to a
+ * multiple of 4 bytes.  Work is queued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream); the call returns after the work completes and
+ * the device status word has been checked. */
+int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, void* stream,
+    double* device_seconds, char* err, size_t err_len);
+
+/* Seeded synthetic permutations used by the benchmark and the tests
+ * (workload generator, not part of the reference).  kind: 0 Fisher-Yates
+ * uniform, 1 Sattolo single cycle, 2 identity, 3 reverse, 4 bit reversal
+ * (count must be a power of two).  Randomness: xoshiro256** seeded from
+ * splitmix64(seed), bounded draws by Lemire's multiply-shift with rejection.
+ * `out` holds count values of entry_bytes (4 or 8). */
+int bpb200_fill_permutation(uint32_t kind, uint64_t seed, uint64_t count,
+    uint32_t entry_bytes, void* out);
+
+/* Releases cached device workspaces (no reference counterpart). */
+void bpb200_shutdown(void);
+
+/* Address probes of the closed-form layout (test hooks, no device work):
+ * section-relative bit of switch `pair` of node `node` at routing level
+ * `level` (side 0 input, 1 output), and the first rank bit of leaf `node`
+ * with its section (0 input, 1 output, 2 middle).  They restate
+ * SectionAddress::switch_bit / middle_bit (src/internal.hpp:486-517). */
+int bpb200_probe_switch_bit(uint64_t count, const bpb200_format* format, int side,
+    uint32_t level, uint64_t node, uint64_t pair, uint64_t* bit);
+int bpb200_probe_rank_bit(uint64_t count, const bpb200_format* format, uint32_t level,
+    uint64_t node, int* section, uint64_t* bit);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BENES_B200_H */

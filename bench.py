@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+# SPDX-License-Identifier: Apache-2.0
+"""Benchmark of the B200 compact encoder (one JSON line on rank 0).
+
+Workload: a uniform random permutation of N = 2^30 uint64 entries (Fisher-
+Yates driven by xoshiro256** seeded through splitmix64), middle_group_log2 5,
+the balanced default clusters and embedded_output middle placement: the
+configuration the headline metric is quoted on.  A step is one full compress
+of that permutation.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+``value``: entries/s with the input already in HBM (device-resident entry
+point), timed with CUDA events on the launching stream over exactly K steps,
+max over ranks.  ``e2e``: the same metric through the host entry point,
+including the host->device copy of the input from pinned memory and the
+device->host copy of the blob.  The path does not shard: with N GPUs every
+rank compresses its own permutation (replicas, weak scaling).
+``--impl reference`` times the reference's portable_cpu encoder (built from
+its own sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "entries/sec compressed bit-exact at N=2^30; serving p50/p99 latency vs plain"
+UNIT = "entries/s"
+SEED = 0x5EED_2030
+CPU_SAMPLE_N = 1 << 23
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    ap.add_argument("--log2n", type=int, default=30, help="workload size (default 30)")
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(log2n):
+    import benes_perm_b200 as bp
+    fmt = bp.FormatOptions(middle_group_log2=5, middle_placement=bp.MiddlePlacement.embedded_output)
+    return 1 << log2n, fmt
+
+
+def workload_config(n, log2n, world):
+    return {
+        "workload": f"compress uniform random permutation, N=2^{log2n} uint64, m=5, "
+                    "default clusters, embedded_output",
+        "n": n, "entry_bytes": 8, "middle_group_log2": 5, "clusters": "balanced default",
+        "middle_placement": "embedded_output",
+        "permutation": "Fisher-Yates, xoshiro256** seeded by splitmix64(0x5EED2030)",
+        "l2": "inputs larger than L2 (8 GiB per step), no flush",
+        "parallelism": f"replicas x{world} (the path does not shard)",
+    }
+
+
+def dist_setup(gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------- roofline
+
+def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits):
+    """Compulsory HBM bytes per kernel kind for one compress (each input read
+    once and each output written once at its minimal width)."""
+    per = {k: 0.0 for k in ("inverse", "union", "resolve", "output_bits", "tile")}
+    for lvl in range(tile):
+        w = entry_bytes if lvl == 0 else 4
+        per["inverse"] += (w + 4) * n             # read values, write inverse
+        per["union"] += 8 * n                      # read inverse, one word per pair read+written
+        per["resolve"] += (2 + w + 4) * n + n / 8  # union-find words, values, children, bits
+        per["output_bits"] += 2 * n + n / 8        # even inverse entries, bits
+    w = entry_bytes if tile == 0 else 4
+    per["tile"] = w * n + 2 * (depth - tile) * n / 16 + middle_bits / 8
+    pipeline = (entry_bytes * n + 4 * n * max(depth - 1, 0) + 4 * n * depth
+                + 2 * switch_bits / 8 + 4 * n + middle_bits / 8)
+    return per, pipeline
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- arms
+
+def reference_arm(args, world, rank):
+    """portable_cpu of the reference on the host cores, bounded sample."""
+    if rank != 0:
+        return
+    from oracle.oracle import Reference, make_format
+    import benes_perm_b200 as bp
+    ref = Reference()
+    threads = ref.hardware_threads()
+    n_sample = CPU_SAMPLE_N
+    perm = bp.fill_permutation(bp.PermutationKind.uniform, SEED, n_sample, np.uint64)
+    fmt = make_format(5, [], [], 2)
+    out = np.zeros(ref.encoded_size(n_sample, fmt), dtype=np.uint8)
+    for _ in range(args.warmup):
+        ref.compress(perm, fmt, threads=threads, out=out)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ref.compress(perm, fmt, threads=threads, out=out)
+    secs = time.perf_counter() - t0
+    value = n_sample * args.steps / secs
+    n, _ = workload(args.log2n)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "uint64", "data": "synthetic",
+        "config": workload_config(n, args.log2n, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"each step compresses a {n_sample}-entry (2^23) uint64 "
+                                   "uniform permutation, same format family, portable_cpu with "
+                                   f"{threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(world):
+    from oracle.oracle import Reference, make_format
+    import benes_perm_b200 as bp
+    ref = Reference()
+    threads = ref.hardware_threads()
+    perm = bp.fill_permutation(bp.PermutationKind.uniform, SEED, CPU_SAMPLE_N, np.uint64)
+    fmt = make_format(5, [], [], 2)
+    out = np.zeros(ref.encoded_size(CPU_SAMPLE_N, fmt), dtype=np.uint8)
+    ref.compress(perm, fmt, threads=threads, out=out)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        ref.compress(perm, fmt, threads=threads, out=out)
+        times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": CPU_SAMPLE_N / med, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"median of 3 compresses of a 2^23-entry uint64 uniform permutation (same "
+                      f"format family) by the reference portable_cpu encoder, {threads} threads"}
+
+
+def b200_arm(args, world, rank, local):
+    import torch
+    import benes_perm_b200 as bp
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    n, fmt = workload(args.log2n)
+    size = bp.encoded_size(n, fmt)
+    depth, tile = bp.describe(n, fmt)
+
+    host = torch.empty(n, dtype=torch.int64, pin_memory=True)
+    perm = host.numpy().view(np.uint64)
+    bp.fill_permutation(bp.PermutationKind.uniform, SEED + rank, n, np.uint64, out=perm)
+    d_in = host.to(f"cuda:{local}", non_blocking=False)
+    d_blob = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return bp.compress_device(d_in.data_ptr(), n, 8, d_blob.data_ptr(), size, fmt,
+                                  stream.cuda_stream)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    _, _, launches_per_step = bp.last_profile()
+
+    gpu_index = local
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    if vis and vis.split(",")[local].strip().isdigit():
+        gpu_index = int(vis.split(",")[local])
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_index) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            step()
+        stop.record(stream)
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    secs = start.elapsed_time(stop) / 1e3
+    if dist is not None:
+        t = torch.tensor([secs], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        secs = float(t.item())
+    value = n * args.steps * world / secs
+
+    # per-kernel device times (separate, untimed pass)
+    bp.set_profiling(True)
+    step()
+    kernel_secs, kernel_counts, _ = bp.last_profile()
+    bp.set_profiling(False)
+
+    # end to end through the host entry point: pinned input in, pinned blob out
+    host_blob = torch.empty(size, dtype=torch.uint8, pin_memory=True)
+    blob_np = host_blob.numpy()
+    opts = bp.CompressOptions(format=fmt)
+    bp.compress(perm, opts, out=blob_np)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        bp.compress(perm, opts, out=blob_np)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_secs = e0.elapsed_time(e1) / 1e3
+    if dist is not None:
+        t = torch.tensor([e2e_secs], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_secs = float(t.item())
+    e2e_value = n * args.e2e_steps * world / e2e_secs
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # roofline of the dominant kernel kind
+    lay_switch = None
+    from benes_perm_b200 import library  # noqa: F401
+    switch_bits, middle_bits = _section_bits(n, fmt)
+    alg, pipeline_bytes = algorithmic_bytes(n, depth, tile, 8, switch_bits, middle_bits)
+    timed = {k: v for k, v in kernel_secs.items() if k in alg and v > 0}
+    dominant = max(timed, key=timed.get)
+    peak, peak_kind = load_peaks()
+    achieved = alg[dominant] / timed[dominant] / 1e9
+    total_kernel = sum(kernel_secs.values())
+    roofline = {
+        "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
+        "traffic": None,
+        "algorithmic_bytes_per_step": alg[dominant],
+        "kernel_seconds_per_step": timed[dominant],
+        "share_of_device_time": timed[dominant] / total_kernel,
+    }
+    pipeline = {
+        "algorithmic_bytes": pipeline_bytes, "seconds": secs / args.steps,
+        "achieved": pipeline_bytes / (secs / args.steps) / 1e9, "peak": peak, "unit": "GB/s",
+        "frac": pipeline_bytes / (secs / args.steps) / 1e9 / peak,
+    }
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": secs / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint64",
+        "data": "synthetic", "config": workload_config(n, args.log2n, world),
+        "clocks": clocks.summary(),
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 8,
+                "d2h_bytes_per_step": size, "steps": args.e2e_steps},
+        "gpu_launches": launches_per_step * args.steps,
+        "roofline": roofline,
+        "pipeline_roofline": pipeline,
+        "kernel_seconds": {k: round(v, 6) for k, v in kernel_secs.items()},
+        "kernel_launches": kernel_counts,
+        "levels": {"depth": depth, "tile_level": tile},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(world)
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def _section_bits(n, fmt):
+    """Switch bits per side and middle bits of the layout (FormatSizeCache)."""
+    leaf = 1 << fmt.middle_group_log2
+    memo = {}
+
+    def fbits(c):
+        f = 1
+        for i in range(2, c + 1):
+            f *= i
+        return (f - 1).bit_length()
+
+    def sizes(c):
+        if c <= leaf:
+            return 0, fbits(c)
+        if c in memo:
+            return memo[c]
+        a = sizes(c - c // 2)
+        b = sizes(c // 2)
+        memo[c] = (c // 2 + a[0] + b[0], a[1] + b[1])
+        return memo[c]
+
+    return sizes(n)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args.gpus)
+    if args.impl == "reference":
+        reference_arm(args, world, rank)
+    else:
+        b200_arm(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

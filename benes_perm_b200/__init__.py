@@ -133,6 +133,13 @@ def library() -> ctypes.CDLL:
                                               ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_uint64)]
         lib.bpb200_shutdown.restype = None
+        lib.bpb200_set_profiling.argtypes = [ctypes.c_int]
+        lib.bpb200_set_profiling.restype = None
+        lib.bpb200_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_uint32), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_uint32)]
+        lib.bpb200_describe.argtypes = [ctypes.c_uint64, fp, ctypes.POINTER(ctypes.c_uint32),
+                                        ctypes.POINTER(ctypes.c_uint32)]
         _lib = lib
     return _lib
 
@@ -178,11 +185,14 @@ def last_device_seconds() -> float:
     return _last_device_seconds
 
 
-def compress(permutation, options: Optional[CompressOptions] = None) -> bytes:
+def compress(permutation, options: Optional[CompressOptions] = None,
+             out: Optional[np.ndarray] = None):
     """benes::compress(span<const uint32_t|uint64_t>, {.backend = b200, ...}).
 
-    ``permutation`` is a 1-D numpy array (or buffer-protocol object) of
-    uint32 or uint64 values.  Returns the canonical version-1 blob.
+    ``permutation`` is a 1-D numpy array of uint32 or uint64 values.  Returns
+    the canonical version-1 blob as ``bytes``; when ``out`` (a uint8 array of
+    at least the encoded size, e.g. a view of pinned memory) is given, the
+    blob is written there and the used slice of ``out`` is returned instead.
     """
     global _last_device_seconds
     options = options or CompressOptions()
@@ -197,7 +207,12 @@ def compress(permutation, options: Optional[CompressOptions] = None) -> bytes:
         raise ValueError("permutation size is out of range")
     raise_for(library().bpb200_encoded_size(n, ctypes.byref(cf), ctypes.byref(size), err, 512),
               err.value.decode())
-    blob = np.empty(size.value, dtype=np.uint8)
+    if out is not None:
+        if out.dtype != np.uint8 or out.size < size.value or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous uint8 array of the encoded size")
+        blob = out[:size.value]
+    else:
+        blob = np.empty(size.value, dtype=np.uint8)
     secs = ctypes.c_double(0)
     rc = library().bpb200_compress(
         arr.ctypes.data, n, arr.dtype.itemsize, ctypes.byref(cf),
@@ -205,7 +220,38 @@ def compress(permutation, options: Optional[CompressOptions] = None) -> bytes:
         ctypes.byref(secs), err, 512)
     raise_for(rc, err.value.decode())
     _last_device_seconds = secs.value
-    return blob.tobytes()
+    return blob if out is not None else blob.tobytes()
+
+
+KERNEL_KINDS = ("prologue", "inverse", "descriptors", "union", "orient", "resolve",
+                "output_bits", "tile")
+
+
+def set_profiling(enabled: bool) -> None:
+    """Bracket every kernel launch of later calls with CUDA events."""
+    library().bpb200_set_profiling(1 if enabled else 0)
+
+
+def last_profile():
+    """(seconds by kernel kind, launches by kernel kind, total launches) of
+    the calling thread's last compress call."""
+    k = len(KERNEL_KINDS)
+    secs = (ctypes.c_double * k)()
+    counts = (ctypes.c_uint32 * k)()
+    total = ctypes.c_uint32(0)
+    library().bpb200_last_profile(secs, counts, k, ctypes.byref(total))
+    return ({KERNEL_KINDS[i]: secs[i] for i in range(k)},
+            {KERNEL_KINDS[i]: counts[i] for i in range(k)}, total.value)
+
+
+def describe(count: int, fmt: Optional[FormatOptions] = None):
+    """(routing depth, first tile level) of the encode for (count, fmt)."""
+    cf = to_c_format(fmt)
+    d = ctypes.c_uint32(0)
+    t = ctypes.c_uint32(0)
+    raise_for(library().bpb200_describe(count, ctypes.byref(cf), ctypes.byref(d),
+                                        ctypes.byref(t)), "invalid format")
+    return d.value, t.value
 
 
 def compress_device(d_entries: int, count: int, entry_bytes: int, d_blob: int, blob_len: int,

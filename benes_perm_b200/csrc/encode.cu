@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -29,6 +30,19 @@ namespace {
 constexpr uint64_t kTileMaxEntries = 8192;
 constexpr uint32_t kTileSmemBudget = 200 * 1024;
 constexpr int kLevelThreads = 256;
+
+// Kernel kinds reported by bpb200_last_profile.
+enum KernelKind : int {
+    kKindPrologue = 0,
+    kKindInverse,
+    kKindDescriptors,
+    kKindUnion,
+    kKindOrient,
+    kKindResolve,
+    kKindOutputBits,
+    kKindTile,
+    kKernelKinds
+};
 
 struct CudaFail {
     cudaError_t err;
@@ -61,6 +75,7 @@ struct Workspace {
     uint64_t input_cap = 0;
     uint32_t* blob = nullptr;     // staging for host-path blobs
     uint64_t blob_cap = 0;
+    std::vector<cudaEvent_t> events; // profiling events, reused across calls
     bool busy = false;
 
     void release_scratch() {
@@ -83,6 +98,7 @@ struct Workspace {
         if (start) cudaEventDestroy(start);
         if (stop) cudaEventDestroy(stop);
         if (stream) cudaStreamDestroy(stream);
+        for (cudaEvent_t e : events) cudaEventDestroy(e);
         *this = Workspace();
     }
 };
@@ -217,10 +233,51 @@ int grid_for(uint64_t work, int threads) {
     return (int)std::max<uint64_t>(1, std::min<uint64_t>(want, cap));
 }
 
+// Optional per-kernel timing: when enabled, every launch is bracketed by a
+// pair of events and the per-kind totals are reported after the call.
+struct Recorder {
+    bool enabled = false;
+    std::vector<cudaEvent_t>* pool = nullptr;
+    std::vector<std::pair<int, size_t>> marks; // (kind, first event index)
+    uint32_t launches = 0;
+    cudaStream_t st = nullptr;
+    size_t used = 0;
+
+    cudaEvent_t next() {
+        if (used == pool->size()) {
+            cudaEvent_t e;
+            check(cudaEventCreate(&e), "cudaEventCreate");
+            pool->push_back(e);
+        }
+        return (*pool)[used++];
+    }
+    template <typename F>
+    void launch(int kind, F&& f) {
+        ++launches;
+        if (!enabled) {
+            f();
+            return;
+        }
+        const size_t i = used;
+        check(cudaEventRecord(next(), st), "cudaEventRecord");
+        f();
+        check(cudaEventRecord(next(), st), "cudaEventRecord");
+        marks.push_back({kind, i});
+    }
+    void collect(double* seconds, uint32_t* counts) {
+        for (auto& m : marks) {
+            float ms = 0;
+            check(cudaEventElapsedTime(&ms, (*pool)[m.second], (*pool)[m.second + 1]),
+                "cudaEventElapsedTime");
+            seconds[m.first] += ms * 1e-3;
+            counts[m.first] += 1;
+        }
+    }
+};
+
 template <typename T>
-void launch_levels(Workspace& w, const Plan& p, const TileShape& shape, const T* d_in,
-    uint32_t* d_blob) {
-    cudaStream_t st = w.stream;
+void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
+    const TileShape& shape, const T* d_in, uint32_t* d_blob) {
     const Plan* dp = w.d_plan;
     const uint32_t t0 = p.tile_level;
     if (t0 > 0) {
@@ -238,23 +295,37 @@ void launch_levels(Workspace& w, const Plan& p, const TileShape& shape, const T*
         const int gs = grid_for(slots, kLevelThreads);
         const int gp = grid_for(prs, kLevelThreads);
         const int gn = grid_for(nodes, kLevelThreads);
-        if (l == 0) {
-            level_inverse<T><<<gs, kLevelThreads, 0, st>>>(dp, l, d_in, w.inv, w.uf, w.d_status);
-        } else {
-            level_inverse<uint32_t><<<gs, kLevelThreads, 0, st>>>(dp, l, cur32, w.inv, w.uf,
-                w.d_status);
-        }
-        level_descriptors<<<gn, kLevelThreads, 0, st>>>(dp, l, w.addr[0], w.addr[1]);
-        level_union<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
-        level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
-        if (l == 0) {
-            level_resolve<T><<<gp, kLevelThreads, 0, st>>>(dp, l, d_in, w.uf, w.xbits, dst,
-                w.addr[0], d_blob, w.d_status);
-        } else {
-            level_resolve<uint32_t><<<gp, kLevelThreads, 0, st>>>(dp, l, cur32, w.uf, w.xbits,
-                dst, w.addr[0], d_blob, w.d_status);
-        }
-        level_output_bits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.addr[1], d_blob);
+        rec.launch(kKindInverse, [&] {
+            if (l == 0) {
+                level_inverse<T><<<gs, kLevelThreads, 0, st>>>(dp, l, d_in, w.inv, w.uf,
+                    w.d_status);
+            } else {
+                level_inverse<uint32_t><<<gs, kLevelThreads, 0, st>>>(dp, l, cur32, w.inv, w.uf,
+                    w.d_status);
+            }
+        });
+        rec.launch(kKindDescriptors, [&] {
+            level_descriptors<<<gn, kLevelThreads, 0, st>>>(dp, l, w.addr[0], w.addr[1]);
+        });
+        rec.launch(kKindUnion, [&] {
+            level_union<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
+        });
+        rec.launch(kKindOrient, [&] {
+            level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
+        });
+        rec.launch(kKindResolve, [&] {
+            if (l == 0) {
+                level_resolve<T><<<gp, kLevelThreads, 0, st>>>(dp, l, d_in, w.uf, w.xbits, dst,
+                    w.addr[0], d_blob, w.d_status);
+            } else {
+                level_resolve<uint32_t><<<gp, kLevelThreads, 0, st>>>(dp, l, cur32, w.uf,
+                    w.xbits, dst, w.addr[0], d_blob, w.d_status);
+            }
+        });
+        rec.launch(kKindOutputBits, [&] {
+            level_output_bits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.addr[1],
+                d_blob);
+        });
         check(cudaGetLastError(), "level kernel launch");
         cur32 = dst;
     }
@@ -265,14 +336,18 @@ void launch_levels(Workspace& w, const Plan& p, const TileShape& shape, const T*
     if (t0 == 0) {
         check(cudaFuncSetAttribute(tile_encode<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                   (int)shape.smem), "cudaFuncSetAttribute");
-        tile_encode<T><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, d_in, d_blob,
-            w.d_status, shape.slots, shape.pairs);
+        rec.launch(kKindTile, [&] {
+            tile_encode<T><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, d_in, d_blob,
+                w.d_status, shape.slots, shape.pairs);
+        });
     } else {
         check(cudaFuncSetAttribute(tile_encode<uint32_t>,
                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape.smem),
             "cudaFuncSetAttribute");
-        tile_encode<uint32_t><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, cur32,
-            d_blob, w.d_status, shape.slots, shape.pairs);
+        rec.launch(kKindTile, [&] {
+            tile_encode<uint32_t><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, cur32,
+                d_blob, w.d_status, shape.slots, shape.pairs);
+        });
     }
     check(cudaGetLastError(), "tile kernel launch");
 }
@@ -345,12 +420,22 @@ int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
     return kOk;
 }
 
-// Queues the whole encode on w.stream and waits for it.
-int run(Workspace& w, Call& call, const void* d_in, uint32_t entry_bytes, uint32_t* d_blob,
-    double* device_seconds, char* err, size_t err_len) {
+// Per-thread record of the last call (the reference keeps device seconds
+// thread_local too, src/benes.cpp:24).
+thread_local double t_kernel_seconds[kKernelKinds];
+thread_local uint32_t t_kernel_counts[kKernelKinds];
+thread_local uint32_t t_launches = 0;
+std::atomic<int> g_profiling{0};
+
+// Queues the whole encode on `st` and waits for it.
+int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t entry_bytes,
+    uint32_t* d_blob, double* device_seconds, char* err, size_t err_len) {
     const Plan& p = *call.plan;
     ensure_scratch(w, p);
-    cudaStream_t st = w.stream;
+    Recorder rec;
+    rec.enabled = g_profiling.load() != 0;
+    rec.pool = &w.events;
+    rec.st = st;
     check(cudaMemcpyAsync(w.d_plan, w.h_plan, sizeof(Plan), cudaMemcpyHostToDevice, st),
         "plan upload");
     Header h{};
@@ -358,11 +443,11 @@ int run(Workspace& w, Call& call, const void* d_in, uint32_t entry_bytes, uint32
     write_header(call.layout, h.data);
     check(cudaEventRecord(w.start, st), "cudaEventRecord");
     check(cudaMemsetAsync(d_blob, 0, (p.end_offset + 3) / 4 * 4, st), "cudaMemsetAsync(blob)");
-    prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h);
+    rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h); });
     if (entry_bytes == 4) {
-        launch_levels<uint32_t>(w, p, call.shape, (const uint32_t*)d_in, d_blob);
+        launch_levels<uint32_t>(w, rec, st, p, call.shape, (const uint32_t*)d_in, d_blob);
     } else {
-        launch_levels<uint64_t>(w, p, call.shape, (const uint64_t*)d_in, d_blob);
+        launch_levels<uint64_t>(w, rec, st, p, call.shape, (const uint64_t*)d_in, d_blob);
     }
     check(cudaEventRecord(w.stop, st), "cudaEventRecord");
     check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
@@ -372,6 +457,12 @@ int run(Workspace& w, Call& call, const void* d_in, uint32_t entry_bytes, uint32
     if (device_seconds) {
         *device_seconds = ms * 1e-3;
     }
+    for (int k = 0; k < kKernelKinds; ++k) {
+        t_kernel_seconds[k] = 0;
+        t_kernel_counts[k] = 0;
+    }
+    rec.collect(t_kernel_seconds, t_kernel_counts);
+    t_launches = rec.launches;
     const uint32_t status = *w.h_status;
     if (status & kErrNotPermutation) {
         set_error(err, err_len, "input must contain every value from zero through size minus one");
@@ -472,7 +563,7 @@ int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
         }
         check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
             "input upload");
-        rc = run(w, call, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
+        rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
         if (rc != kOk) {
             return rc;
         }
@@ -503,17 +594,40 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
         if (rc != kOk) {
             return rc;
         }
-        cudaStream_t user = (cudaStream_t)stream;
-        // order the workspace stream after the caller's prior work, and the
-        // caller's later work after ours
-        cudaEvent_t ev;
-        check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
-        check(cudaEventRecord(ev, user), "cudaEventRecord");
-        check(cudaStreamWaitEvent(w.stream, ev, 0), "cudaStreamWaitEvent");
-        rc = run(w, call, d_entries, entry_bytes, (uint32_t*)d_blob, device_seconds, err, err_len);
-        cudaEventDestroy(ev);
-        return rc;
+        // the work is queued on the caller's stream, after its earlier work
+        return run(w, call, (cudaStream_t)stream, d_entries, entry_bytes, (uint32_t*)d_blob,
+            device_seconds, err, err_len);
     });
+}
+
+void bpb200_set_profiling(int enabled) { g_profiling.store(enabled ? 1 : 0); }
+
+int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth,
+    uint32_t* tile_level) {
+    Layout L;
+    const Error e = make_layout(count, to_format(format), &L);
+    if (!e.ok()) {
+        return e.code;
+    }
+    std::unique_ptr<Plan> p(new Plan);
+    if (!make_plan(L, kTileMaxEntries, p.get()).ok()) {
+        return kLength;
+    }
+    TileShape shape;
+    choose_tile(*p, &shape);
+    if (depth) *depth = p->depth;
+    if (tile_level) *tile_level = p->tile_level;
+    return kOk;
+}
+
+int bpb200_last_profile(double* seconds, uint32_t* launches, int kinds, uint32_t* total_launches) {
+    const int n = kinds < kKernelKinds ? kinds : kKernelKinds;
+    for (int k = 0; k < n; ++k) {
+        if (seconds) seconds[k] = t_kernel_seconds[k];
+        if (launches) launches[k] = t_kernel_counts[k];
+    }
+    if (total_launches) *total_launches = t_launches;
+    return kKernelKinds;
 }
 
 void bpb200_shutdown(void) {

@@ -87,6 +87,23 @@ int bpb200_fill_permutation(uint32_t kind, uint64_t seed, uint64_t count,
 /* Releases cached device workspaces (no reference counterpart). */
 void bpb200_shutdown(void);
 
+/* Per-kernel device timing (tracing hook; the reference only records total
+ * device seconds, src/benes.cpp:119-125).  When enabled, every kernel launch
+ * of later calls is bracketed by CUDA events.  bpb200_last_profile reports,
+ * for the calling thread's last call, seconds and launch counts per kernel
+ * kind (0 prologue, 1 inverse, 2 descriptors, 3 union, 4 orient, 5 resolve,
+ * 6 output bits, 7 tile) and the total number of kernel launches; it returns
+ * the number of kinds. */
+void bpb200_set_profiling(int enabled);
+
+/* Geometry of the encode the library would run for (count, format): the
+ * routing depth and the first level handled by the shared-memory tile
+ * kernel (levels above it run as global-memory level kernels). */
+int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth,
+    uint32_t* tile_level);
+int bpb200_last_profile(double* seconds, uint32_t* launches, int kinds,
+    uint32_t* total_launches);
+
 /* Address probes of the closed-form layout (test hooks, no device work):
  * section-relative bit of switch `pair` of node `node` at routing level
  * `level` (side 0 input, 1 output), and the first rank bit of leaf `node`

@@ -684,3 +684,154 @@ int bpb200_probe_rank_bit(uint64_t count, const bpb200_format* format, uint32_t 
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot call cudaMalloc: code running while a CUDA stream is
+// being captured into a graph (allocation is not allowed during capture),
+// processes whose device memory is owned by a pooling allocator that must
+// account for every byte, and latency-critical paths that cannot afford the
+// device-wide synchronisation cudaMalloc/cudaFree can imply.  For them,
+// bpb200_compress_device_noalloc runs the same encode with all of its
+// scratch (plan, status word, level arrays, inverse, union-find words,
+// colour bits, node descriptors) carved out of one file-scope device array
+// of fixed size.  The array exists on every GPU that loads this library and
+// stays allocated until the process exits.
+// ---------------------------------------------------------------------------
+namespace bpb200 {
+namespace noalloc {
+
+constexpr uint64_t kMaxEntries = 1ull << 18;          // largest permutation accepted
+constexpr uint64_t kSlots = kMaxEntries + (1ull << 14); // level slots incl. padding
+constexpr uint64_t kPairs = kSlots / 2 + (1ull << 13);
+constexpr uint64_t kNodes = 1ull << 10;               // descriptors per global level
+
+constexpr size_t up256(size_t x) { return (x + 255) / 256 * 256; }
+constexpr size_t kOffPlan = 0;
+constexpr size_t kOffStatus = kOffPlan + up256(sizeof(Plan));
+constexpr size_t kOffVals0 = kOffStatus + 256;
+constexpr size_t kOffVals1 = kOffVals0 + up256(kSlots * 4);
+constexpr size_t kOffInv = kOffVals1 + up256(kSlots * 4);
+constexpr size_t kOffUf = kOffInv + up256(kSlots * 4);
+constexpr size_t kOffXbits = kOffUf + up256(kPairs * 4);
+constexpr size_t kOffAddr0 = kOffXbits + up256((kPairs / 32 + 1) * 4);
+constexpr size_t kOffAddr1 = kOffAddr0 + up256(kNodes * sizeof(NodeAddress));
+constexpr size_t kBytes = kOffAddr1 + up256(kNodes * sizeof(NodeAddress)); // about 4.5 MB
+
+} // namespace noalloc
+} // namespace bpb200
+
+// The scratch itself.  In host code this name is only a host-side stand-in,
+// not a device address; the device address is obtained per device with
+// cudaGetSymbolAddress below.
+static __device__ __align__(256) unsigned char bpb200_noalloc_scratch[bpb200::noalloc::kBytes];
+
+namespace bpb200 {
+namespace noalloc {
+
+constexpr int kMaxDevices = 64;
+std::mutex g_mutex;                    // guards the two tables below
+unsigned char* g_scratch[kMaxDevices]; // device address of the array, per device
+Plan g_plan;                           // host staging of the plan (no heap, no pinning)
+
+} // namespace noalloc
+} // namespace bpb200
+
+extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t count,
+    uint32_t entry_bytes, const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len,
+    void* stream, char* err, size_t err_len) {
+    using namespace bpb200;
+    return guarded(err, err_len, [&]() -> int {
+        int device = 0;
+        if (!current_device_ok(&device)) {
+            set_error(err, err_len, "b200 backend is unavailable");
+            return kUnavailable;
+        }
+        if (device < 0 || device >= noalloc::kMaxDevices) {
+            set_error(err, err_len, "device ordinal out of range for the allocation-free entry point");
+            return kRuntime;
+        }
+        if (count > noalloc::kMaxEntries) {
+            set_error(err, err_len,
+                "the allocation-free entry point accepts at most 262144 (2^18) entries");
+            return kLength;
+        }
+        if (((uintptr_t)d_blob & 3u) != 0) {
+            set_error(err, err_len, "device blob must be 4-byte aligned");
+            return kInvalidArgument;
+        }
+        // One host thread at a time stages the plan; device-side overlap of
+        // two calls is the caller's to avoid (they would share the scratch).
+        std::lock_guard<std::mutex> lock(noalloc::g_mutex);
+        if (noalloc::g_scratch[device] == nullptr) {
+            // first call on this device: resolve the array's device address
+            // (must happen before any stream capture that uses this entry point)
+            void* ptr = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&ptr, bpb200_noalloc_scratch);
+            if (e != cudaSuccess || ptr == nullptr) {
+                set_error(err, err_len, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+                return kRuntime;
+            }
+            noalloc::g_scratch[device] = static_cast<unsigned char*>(ptr);
+        }
+        unsigned char* base = noalloc::g_scratch[device];
+        Workspace w; // views into the static array; owns nothing
+        w.h_plan = &noalloc::g_plan;
+        Call call;
+        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+        if (rc != kOk) {
+            return rc;
+        }
+        const Plan& p = *call.plan;
+        const uint64_t nodes = p.tile_level > 0 ? (1ull << (p.tile_level - 1)) : 0;
+        if ((p.tile_level > 0 && (p.max_slots > noalloc::kSlots || p.max_pairs > noalloc::kPairs)) ||
+            nodes > noalloc::kNodes) {
+            set_error(err, err_len, "format needs more scratch than the allocation-free entry point holds");
+            return kLength;
+        }
+        w.d_plan = reinterpret_cast<Plan*>(base + noalloc::kOffPlan);
+        w.d_status = reinterpret_cast<uint32_t*>(base + noalloc::kOffStatus);
+        w.vals[0] = reinterpret_cast<uint32_t*>(base + noalloc::kOffVals0);
+        w.vals[1] = reinterpret_cast<uint32_t*>(base + noalloc::kOffVals1);
+        w.inv = reinterpret_cast<uint32_t*>(base + noalloc::kOffInv);
+        w.uf = reinterpret_cast<uint32_t*>(base + noalloc::kOffUf);
+        w.xbits = reinterpret_cast<uint32_t*>(base + noalloc::kOffXbits);
+        w.addr[0] = reinterpret_cast<NodeAddress*>(base + noalloc::kOffAddr0);
+        w.addr[1] = reinterpret_cast<NodeAddress*>(base + noalloc::kOffAddr1);
+        cudaStream_t st = (cudaStream_t)stream;
+        // The plan source is ordinary host memory: the copy is staged before
+        // cudaMemcpyAsync returns, so g_plan can be reused by the next call.
+        check(cudaMemcpyAsync(w.d_plan, &noalloc::g_plan, sizeof(Plan), cudaMemcpyHostToDevice, st),
+            "plan upload");
+        Header h{};
+        h.bytes = (uint32_t)call.layout.header_bytes;
+        write_header(call.layout, h.data);
+        // Everything that must start cleared is cleared by the call itself:
+        // the blob (memset), the status word (prologue) and, when level
+        // kernels run, the inverse sentinels used for validation.
+        check(cudaMemsetAsync(d_blob, 0, (p.end_offset + 3) / 4 * 4, st), "cudaMemsetAsync(blob)");
+        Recorder rec; // timing disabled: no events are created
+        rec.st = st;
+        rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, (uint32_t*)d_blob, h); });
+        if (entry_bytes == 4) {
+            launch_levels<uint32_t>(w, rec, st, p, call.shape, (const uint32_t*)d_entries,
+                (uint32_t*)d_blob);
+        } else {
+            launch_levels<uint64_t>(w, rec, st, p, call.shape, (const uint64_t*)d_entries,
+                (uint32_t*)d_blob);
+        }
+        uint32_t status = 0;
+        check(cudaMemcpyAsync(&status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
+        check(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+        if (status & kErrNotPermutation) {
+            set_error(err, err_len, "input must contain every value from zero through size minus one");
+            return kInvalidArgument;
+        }
+        if (status & (kErrIterationCap | kErrInconsistent)) {
+            set_error(err, err_len, "b200 device status reported a failed colouring");
+            return kRuntime;
+        }
+        return kOk;
+    });
+}

@@ -75,6 +75,27 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
     const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, void* stream,
     double* device_seconds, char* err, size_t err_len);
 
+/* Allocation-free form of bpb200_compress_device.  No counterpart in the
+ * reference: its backends all allocate per call.  For callers that cannot
+ * call cudaMalloc — code that runs while a stream is being captured into a
+ * CUDA graph, processes whose device memory belongs to a pooling allocator,
+ * latency-critical paths that must not trigger the synchronisation an
+ * allocation can imply.  Same arguments and result bytes as
+ * bpb200_compress_device (device input and blob, work queued on `stream`),
+ * but every byte of scratch comes from one fixed device array inside this
+ * library (about 4.5 MB, present on every GPU that loads the library until
+ * the process exits), so it accepts at most 262144 (2^18) entries and
+ * returns BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before capturing a stream
+ * that uses this entry point.  All calls share the one array: calls whose
+ * GPU work overlaps (different streams or host threads without ordering)
+ * race and corrupt each other's results.  Each call clears what it needs
+ * cleared (blob, status word, validation sentinels). */
+int bpb200_compress_device_noalloc(const void* d_entries, uint64_t count,
+    uint32_t entry_bytes, const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len,
+    void* stream, char* err, size_t err_len);
+
 /* Seeded synthetic permutations used by the benchmark and the tests
  * (workload generator, not part of the reference).  kind: 0 Fisher-Yates
  * uniform, 1 Sattolo single cycle, 2 identity, 3 reverse, 4 bit reversal

@@ -140,6 +140,9 @@ def library() -> ctypes.CDLL:
                                             ctypes.POINTER(ctypes.c_uint32)]
         lib.bpb200_describe.argtypes = [ctypes.c_uint64, fp, ctypes.POINTER(ctypes.c_uint32),
                                         ctypes.POINTER(ctypes.c_uint32)]
+        lib.bpb200_last_profile_launches.argtypes = [ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.POINTER(ctypes.c_int),
+                                                     ctypes.POINTER(ctypes.c_double), ctypes.c_int]
         _lib = lib
     return _lib
 
@@ -224,12 +227,17 @@ def compress(permutation, options: Optional[CompressOptions] = None,
 
 
 KERNEL_KINDS = ("prologue", "inverse", "descriptors", "union", "orient", "resolve",
-                "output_bits", "tile")
+                "output_bits", "tile", "emit", "walk", "jump")
 
 
 def set_profiling(enabled: bool) -> None:
     """Bracket every kernel launch of later calls with CUDA events."""
     library().bpb200_set_profiling(1 if enabled else 0)
+
+
+def set_union_find_only(enabled: bool) -> None:
+    """Test hook: colour global levels with union-find instead of orbit walks."""
+    library().bpb200_set_colouring(1 if enabled else 0)
 
 
 def last_profile():
@@ -242,6 +250,18 @@ def last_profile():
     library().bpb200_last_profile(secs, counts, k, ctypes.byref(total))
     return ({KERNEL_KINDS[i]: secs[i] for i in range(k)},
             {KERNEL_KINDS[i]: counts[i] for i in range(k)}, total.value)
+
+
+def last_profile_launches():
+    """[(kind name, routing level, seconds)] of every timed launch of the
+    calling thread's last compress call (profiling must be enabled)."""
+    lib = library()
+    n = lib.bpb200_last_profile_launches(None, None, None, 0)
+    kinds = (ctypes.c_int * max(n, 1))()
+    levels = (ctypes.c_int * max(n, 1))()
+    secs = (ctypes.c_double * max(n, 1))()
+    lib.bpb200_last_profile_launches(kinds, levels, secs, n)
+    return [(KERNEL_KINDS[kinds[i]], levels[i], secs[i]) for i in range(n)]
 
 
 def describe(count: int, fmt: Optional[FormatOptions] = None):

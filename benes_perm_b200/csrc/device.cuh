@@ -99,6 +99,123 @@ __device__ __forceinline__ void uf_union(Word* uf, uint32_t a, uint32_t b, uint3
     atomicOr(err, kErrIterationCap);
 }
 
+// K finds advanced in lockstep: every round issues the loads of all
+// unfinished finds before using any of them, so one thread keeps up to 2K
+// independent loads in flight.  Bits of `pending` name the finds to run.
+template <int K, typename Word>
+__device__ __forceinline__ void uf_find_many(Word* uf, const uint32_t (&x)[K], Found (&out)[K],
+    uint32_t pending, uint32_t* err) {
+    uint32_t cur[K], acc[K];
+#pragma unroll
+    for (int i = 0; i < K; ++i) {
+        cur[i] = x[i];
+        acc[i] = 0;
+    }
+    for (uint32_t it = 0; pending != 0; ++it) {
+        if (it == kSpinCap) {
+            atomicOr(err, kErrIterationCap);
+#pragma unroll
+            for (int i = 0; i < K; ++i) {
+                if (pending & (1u << i)) out[i] = {cur[i], acc[i]};
+            }
+            return;
+        }
+        uint32_t w[K], wp[K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (pending & (1u << i)) w[i] = (uint32_t)uf_load(uf, cur[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (pending & (1u << i)) {
+                const uint32_t p = w[i] >> 1;
+                if (p == cur[i]) {
+                    out[i] = {cur[i], acc[i]};
+                    pending &= ~(1u << i);
+                } else {
+                    wp[i] = (uint32_t)uf_load(uf, p);
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (pending & (1u << i)) {
+                const uint32_t p = w[i] >> 1;
+                const uint32_t pp = wp[i] >> 1;
+                if (pp == p) {
+                    out[i] = {p, acc[i] ^ (w[i] & 1u)};
+                    pending &= ~(1u << i);
+                } else {
+                    const uint32_t nb = (w[i] ^ wp[i]) & 1u;
+                    uf[cur[i]] = (Word)((pp << 1) | nb);
+                    acc[i] ^= nb;
+                    cur[i] = pp;
+                }
+            }
+        }
+    }
+}
+
+// K unions x(a[i]) ^ x(b[i]) == rel[i], with all 2K finds of a round in
+// lockstep.  A failed link retries from the two roots it saw.
+template <int K, typename Word>
+__device__ __forceinline__ void uf_union_many(Word* uf, uint32_t (&a)[K], uint32_t (&b)[K],
+    uint32_t (&rel)[K], uint32_t pending, uint32_t* err) {
+    for (uint32_t it = 0; pending != 0; ++it) {
+        if (it == kSpinCap) {
+            atomicOr(err, kErrIterationCap);
+            return;
+        }
+        uint32_t x[2 * K];
+        Found f[2 * K];
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            x[i] = a[i];
+            x[K + i] = b[i];
+        }
+        uint32_t both = 0;
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (pending & (1u << i)) both |= (1u << i) | (1u << (K + i));
+        }
+        uf_find_many<2 * K>(uf, x, f, both, err);
+#pragma unroll
+        for (int i = 0; i < K; ++i) {
+            if (!(pending & (1u << i))) continue;
+            rel[i] ^= f[i].bit ^ f[K + i].bit;
+            a[i] = f[i].root;
+            b[i] = f[K + i].root;
+            if (a[i] == b[i]) {
+                if (rel[i] != 0) atomicOr(err, kErrInconsistent);
+                pending &= ~(1u << i);
+                continue;
+            }
+            const uint32_t lo = a[i] < b[i] ? a[i] : b[i];
+            const uint32_t hi = a[i] < b[i] ? b[i] : a[i];
+            if (cas_word((uint32_t*)(uf + hi), hi << 1, (lo << 1) | rel[i]) == (hi << 1)) {
+                pending &= ~(1u << i);
+            }
+        }
+    }
+}
+
+// Blocks take chunks of `chunk` consecutive items in increasing order from
+// *counter, so the items in flight across the whole GPU stay within a few
+// chunks of each other.  (A grid-stride loop lets blocks drift apart and
+// spreads node-local random accesses over far more memory than L2 holds.)
+// Every thread of the block must call it.
+__device__ __forceinline__ bool claim_chunk(uint32_t* counter, uint64_t chunk, uint64_t total,
+    uint64_t* first) {
+    __shared__ uint64_t s_first;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_first = (uint64_t)atomicAdd(counter, 1u) * chunk;
+    }
+    __syncthreads();
+    *first = s_first;
+    return s_first < total;
+}
+
 // ------------------------------------------------------------------------
 // Warp-aggregated emission of single bits into the blob.  Lanes of the
 // warp named in `active` call it together; each lane with `set` ORs bit

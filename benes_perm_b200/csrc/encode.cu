@@ -12,12 +12,14 @@
 #include "layout.hpp"
 #include "plan.hpp"
 #include "tile.cuh"
+#include "walk.cuh"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -41,6 +43,9 @@ enum KernelKind : int {
     kKindResolve,
     kKindOutputBits,
     kKindTile,
+    kKindEmit,
+    kKindWalk,
+    kKindJump,
     kKernelKinds
 };
 
@@ -69,6 +74,12 @@ struct Workspace {
     uint32_t* inv = nullptr;
     uint32_t* uf = nullptr;
     uint32_t* xbits = nullptr;
+    uint32_t* ybits = nullptr;
+    uint32_t* owner = nullptr;             // ruler id stamped on each walked vertex
+    uint4* state[2] = {nullptr, nullptr};  // ruler states, double-buffered for jumping
+    uint32_t* control = nullptr;           // per-level control words (walk.cuh)
+    uint2* records = nullptr;              // partitioned-inverse records (kernels.cuh)
+    uint32_t* cursor = nullptr;            // fill level of each destination window
     NodeAddress* addr[2] = {nullptr, nullptr};
     uint64_t slot_cap = 0, pair_cap = 0, node_cap = 0;
     void* input = nullptr;        // staging for host-path inputs
@@ -80,10 +91,13 @@ struct Workspace {
 
     void release_scratch() {
         for (void* p : {(void*)vals[0], (void*)vals[1], (void*)inv, (void*)uf, (void*)xbits,
-                 (void*)addr[0], (void*)addr[1]}) {
+                 (void*)ybits, (void*)owner, (void*)state[0], (void*)state[1], (void*)control,
+                 (void*)records, (void*)cursor, (void*)addr[0], (void*)addr[1]}) {
             if (p) cudaFree(p);
         }
-        vals[0] = vals[1] = inv = uf = xbits = nullptr;
+        vals[0] = vals[1] = inv = uf = xbits = ybits = owner = control = cursor = nullptr;
+        records = nullptr;
+        state[0] = state[1] = nullptr;
         addr[0] = addr[1] = nullptr;
         slot_cap = pair_cap = node_cap = 0;
     }
@@ -143,7 +157,9 @@ void ensure_scratch(Workspace& w, const Plan& p) {
     const uint64_t slots = p.tile_level > 0 ? p.max_slots : 0;
     const uint64_t pairs = p.tile_level > 0 ? p.max_pairs : 0;
     const uint64_t nodes = p.tile_level > 0 ? (1ull << (p.tile_level - 1)) : 0;
-    if (slots <= w.slot_cap && pairs <= w.pair_cap && nodes <= w.node_cap) {
+    const bool need_records = p.levels[0].cap > kWalkMaxNode;
+    if (slots <= w.slot_cap && pairs <= w.pair_cap && nodes <= w.node_cap &&
+        (w.records != nullptr || !need_records)) {
         return;
     }
     w.release_scratch();
@@ -155,6 +171,17 @@ void ensure_scratch(Workspace& w, const Plan& p) {
     check(cudaMalloc(&w.inv, slots * 4), "cudaMalloc(inverse)");
     check(cudaMalloc(&w.uf, pairs * 4), "cudaMalloc(union-find)");
     check(cudaMalloc(&w.xbits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(colour bits)");
+    check(cudaMalloc(&w.ybits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(output bits)");
+    check(cudaMalloc(&w.owner, slots * 4), "cudaMalloc(owners)");
+    const uint64_t buckets = (slots >> kRulerLog2) + 1;
+    check(cudaMalloc(&w.state[0], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
+    check(cudaMalloc(&w.state[1], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
+    check(cudaMalloc(&w.control, kCtlWords * 4), "cudaMalloc(control)");
+    if (p.levels[0].cap > kWalkMaxNode) {
+        // only levels with nodes above L2 size use the partitioned inverse
+        check(cudaMalloc(&w.records, slots * sizeof(uint2)), "cudaMalloc(records)");
+        check(cudaMalloc(&w.cursor, kMaxWindows * 4), "cudaMalloc(cursors)");
+    }
     check(cudaMalloc(&w.addr[0], nodes * sizeof(NodeAddress)), "cudaMalloc(descriptors)");
     check(cudaMalloc(&w.addr[1], nodes * sizeof(NodeAddress)), "cudaMalloc(descriptors)");
     w.slot_cap = slots;
@@ -193,7 +220,7 @@ TileShape tile_shape(const Plan& p, uint32_t t0) {
     TileShape s;
     s.slots = (uint32_t)std::min<uint64_t>(slots, 1u << 30);
     s.pairs = (uint32_t)std::min<uint64_t>(pairs, 1u << 30);
-    uint32_t off[7];
+    uint32_t off[8];
     s.smem = tile_smem_layout(s.slots, s.pairs, off);
     if (slots >= 65536 || pairs >= (1u << 30)) {
         s.smem = UINT32_MAX;
@@ -224,6 +251,20 @@ void choose_tile(Plan& p, TileShape* shape) {
     *shape = s;
 }
 
+std::atomic<int> g_force_union_find{0};
+
+// Launch-shape tuning (BPB200_WALK_BLOCKS_PER_SM overrides the default):
+// resident walkers times the slots per ruler is the address window the
+// walks keep live, which must stay inside L2.
+int walk_blocks_per_sm() {
+    static const int value = [] {
+        const char* env = std::getenv("BPB200_WALK_BLOCKS_PER_SM");
+        const int v = env ? std::atoi(env) : 2;
+        return v < 1 ? 1 : (v > 8 ? 8 : v);
+    }();
+    return value;
+}
+
 int grid_for(uint64_t work, int threads) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -238,8 +279,14 @@ int grid_for(uint64_t work, int threads) {
 struct Recorder {
     bool enabled = false;
     std::vector<cudaEvent_t>* pool = nullptr;
-    std::vector<std::pair<int, size_t>> marks; // (kind, first event index)
+    struct Mark {
+        int kind;
+        int level;
+        size_t first; // index of the opening event
+    };
+    std::vector<Mark> marks;
     uint32_t launches = 0;
+    int level = -1; // routing level of the launches being recorded
     cudaStream_t st = nullptr;
     size_t used = 0;
 
@@ -262,18 +309,116 @@ struct Recorder {
         check(cudaEventRecord(next(), st), "cudaEventRecord");
         f();
         check(cudaEventRecord(next(), st), "cudaEventRecord");
-        marks.push_back({kind, i});
+        marks.push_back({kind, level, i});
     }
-    void collect(double* seconds, uint32_t* counts) {
+    void collect(double* seconds, uint32_t* counts, std::vector<Mark>* per_launch,
+        std::vector<double>* per_launch_seconds) {
+        per_launch->clear();
+        per_launch_seconds->clear();
         for (auto& m : marks) {
             float ms = 0;
-            check(cudaEventElapsedTime(&ms, (*pool)[m.second], (*pool)[m.second + 1]),
+            check(cudaEventElapsedTime(&ms, (*pool)[m.first], (*pool)[m.first + 1]),
                 "cudaEventElapsedTime");
-            seconds[m.first] += ms * 1e-3;
-            counts[m.first] += 1;
+            seconds[m.kind] += ms * 1e-3;
+            counts[m.kind] += 1;
+            per_launch->push_back(m);
+            per_launch_seconds->push_back(ms * 1e-3);
         }
     }
 };
+
+// One global routing level: inverse, orbit-walk colouring (union-find only
+// when the walks give up), children, then both sections' switch bits.
+template <typename TV>
+void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint32_t l,
+    const TV* src, uint32_t* dst, uint32_t* d_blob) {
+    const Plan* dp = w.d_plan;
+    const LevelInfo& lv = p.levels[l];
+    const uint64_t slots = lv.cap << l;
+    const uint64_t prs = lv.pcap << l;
+    const uint64_t nodes = 1ull << l;
+    const uint32_t buckets = (uint32_t)((slots + (1u << kRulerLog2) - 1) >> kRulerLog2);
+    const int gs = grid_for((slots + kInverseItems - 1) / kInverseItems, kLevelThreads);
+    const int gu = grid_for((prs + kUnionItems - 1) / kUnionItems, kLevelThreads);
+    const int gr = grid_for((prs + kResolveItems - 1) / kResolveItems, kLevelThreads);
+    const int gp = grid_for(prs, kLevelThreads);
+    const int gn = grid_for(nodes, kLevelThreads);
+    const int gw = grid_for(buckets, kLevelThreads);
+    uint32_t* ctl = w.control;
+    // nodes whose arrays do not fit in L2 are coloured by union-find
+    const bool walks = lv.cap <= kWalkMaxNode && g_force_union_find.load() == 0;
+    control_reset<<<1, 32, 0, st>>>(ctl, walks ? 0u : 1u);
+    if (lv.cap > kWalkMaxNode && w.records != nullptr) {
+        const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
+        check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
+        const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kLevelThreads);
+        rec.launch(kKindInverse, [&] {
+            level_bucket<TV><<<gb, kLevelThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
+                w.d_status);
+            level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
+                w.records, w.cursor, w.inv, ctl + kCtlClaimPlace);
+        });
+    } else {
+        rec.launch(kKindInverse, [&] {
+            level_inverse<TV><<<gs, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.uf, w.owner,
+                ctl + kCtlClaimInverse, w.d_status);
+        });
+    }
+    rec.launch(kKindDescriptors, [&] {
+        level_descriptors<<<gn, kLevelThreads, 0, st>>>(dp, l, w.addr[0], w.addr[1]);
+    });
+    if (walks) {
+        rec.launch(kKindWalk, [&] {
+            // persistent warps claiming ruler chunks in address order
+            int dev = 0, sms = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            const uint64_t want = ((uint64_t)buckets + kWalkChunk - 1) / kWalkChunk * 32;
+            const int gwalk = (int)std::max<uint64_t>(1,
+                std::min<uint64_t>((uint64_t)sms * walk_blocks_per_sm(),
+                    (want + kLevelThreads - 1) / kLevelThreads));
+            level_walk<TV><<<gwalk, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner,
+                w.state[0], ctl);
+            level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner, ctl);
+        });
+        // rulers of one orbit lie in one node: at most cap/32 + 2 of them
+        uint32_t rounds = 1;
+        while ((1ull << rounds) < (lv.cap >> kRulerLog2) + 2) {
+            ++rounds;
+        }
+        rec.launch(kKindJump, [&] {
+            for (uint32_t r = 0; r <= rounds; ++r) {
+                ruler_jump<<<gw, kLevelThreads, 0, st>>>(w.state[r & 1], w.state[(r + 1) & 1],
+                    buckets, r, ctl);
+                ruler_check<<<1, 1, 0, st>>>(r, ctl);
+            }
+        });
+    }
+    rec.launch(kKindUnion, [&] {
+        level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
+    });
+    rec.launch(kKindOrient, [&] {
+        level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
+    });
+    rec.launch(kKindResolve, [&] {
+        level_finalize<TV><<<gr, kLevelThreads, 0, st>>>(dp, l, src, w.owner, w.state[0],
+            w.state[1], w.uf, w.xbits, dst, ctl, w.d_status);
+    });
+    rec.launch(kKindOutputBits, [&] {
+        level_ybits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.ybits);
+    });
+    for (int side = 0; side < 2; ++side) {
+        const LevelSide& ls = lv.side[side];
+        const uint32_t span_log2 = p.groups[side][ls.group].depth - ls.rel - 1;
+        const uint64_t packets = (lv.cap / 2 + (1ull << span_log2) - 1) >> span_log2;
+        const int ge = grid_for(packets << (l + span_log2), kLevelThreads);
+        rec.launch(kKindEmit, [&] {
+            level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, side == 0 ? w.xbits : w.ybits,
+                w.addr[side], d_blob);
+        });
+    }
+    check(cudaGetLastError(), "level kernel launch");
+}
 
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
@@ -287,48 +432,16 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     }
     const uint32_t* cur32 = nullptr;
     for (uint32_t l = 0; l < t0; ++l) {
-        const LevelInfo& lv = p.levels[l];
-        const uint64_t slots = lv.cap << l;
-        const uint64_t prs = lv.pcap << l;
-        const uint64_t nodes = 1ull << l;
+        rec.level = (int)l;
         uint32_t* dst = w.vals[l & 1];
-        const int gs = grid_for(slots, kLevelThreads);
-        const int gp = grid_for(prs, kLevelThreads);
-        const int gn = grid_for(nodes, kLevelThreads);
-        rec.launch(kKindInverse, [&] {
-            if (l == 0) {
-                level_inverse<T><<<gs, kLevelThreads, 0, st>>>(dp, l, d_in, w.inv, w.uf,
-                    w.d_status);
-            } else {
-                level_inverse<uint32_t><<<gs, kLevelThreads, 0, st>>>(dp, l, cur32, w.inv, w.uf,
-                    w.d_status);
-            }
-        });
-        rec.launch(kKindDescriptors, [&] {
-            level_descriptors<<<gn, kLevelThreads, 0, st>>>(dp, l, w.addr[0], w.addr[1]);
-        });
-        rec.launch(kKindUnion, [&] {
-            level_union<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
-        });
-        rec.launch(kKindOrient, [&] {
-            level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, w.d_status);
-        });
-        rec.launch(kKindResolve, [&] {
-            if (l == 0) {
-                level_resolve<T><<<gp, kLevelThreads, 0, st>>>(dp, l, d_in, w.uf, w.xbits, dst,
-                    w.addr[0], d_blob, w.d_status);
-            } else {
-                level_resolve<uint32_t><<<gp, kLevelThreads, 0, st>>>(dp, l, cur32, w.uf,
-                    w.xbits, dst, w.addr[0], d_blob, w.d_status);
-            }
-        });
-        rec.launch(kKindOutputBits, [&] {
-            level_output_bits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.addr[1],
-                d_blob);
-        });
-        check(cudaGetLastError(), "level kernel launch");
+        if (l == 0) {
+            run_level<T>(w, rec, st, p, l, d_in, dst, d_blob);
+        } else {
+            run_level<uint32_t>(w, rec, st, p, l, cur32, dst, d_blob);
+        }
         cur32 = dst;
     }
+    rec.level = (int)t0;
     const uint64_t tiles = 1ull << t0;
     if (tiles > 0x7fffffffull) {
         throw CudaFail{cudaErrorInvalidValue, "too many tiles"};
@@ -425,6 +538,8 @@ int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
 thread_local double t_kernel_seconds[kKernelKinds];
 thread_local uint32_t t_kernel_counts[kKernelKinds];
 thread_local uint32_t t_launches = 0;
+thread_local std::vector<Recorder::Mark> t_marks;
+thread_local std::vector<double> t_mark_seconds;
 std::atomic<int> g_profiling{0};
 
 // Queues the whole encode on `st` and waits for it.
@@ -461,7 +576,7 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
         t_kernel_seconds[k] = 0;
         t_kernel_counts[k] = 0;
     }
-    rec.collect(t_kernel_seconds, t_kernel_counts);
+    rec.collect(t_kernel_seconds, t_kernel_counts, &t_marks, &t_mark_seconds);
     t_launches = rec.launches;
     const uint32_t status = *w.h_status;
     if (status & kErrNotPermutation) {
@@ -602,6 +717,8 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
 
 void bpb200_set_profiling(int enabled) { g_profiling.store(enabled ? 1 : 0); }
 
+void bpb200_set_colouring(int union_find_only) { g_force_union_find.store(union_find_only ? 1 : 0); }
+
 int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth,
     uint32_t* tile_level) {
     Layout L;
@@ -618,6 +735,16 @@ int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth
     if (depth) *depth = p->depth;
     if (tile_level) *tile_level = p->tile_level;
     return kOk;
+}
+
+int bpb200_last_profile_launches(int* kinds, int* levels, double* seconds, int capacity) {
+    const int n = (int)t_marks.size();
+    for (int i = 0; i < n && i < capacity; ++i) {
+        if (kinds) kinds[i] = t_marks[i].kind;
+        if (levels) levels[i] = t_marks[i].level;
+        if (seconds) seconds[i] = t_mark_seconds[i];
+    }
+    return n;
 }
 
 int bpb200_last_profile(double* seconds, uint32_t* launches, int kinds, uint32_t* total_launches) {
@@ -715,9 +842,14 @@ constexpr size_t kOffVals1 = kOffVals0 + up256(kSlots * 4);
 constexpr size_t kOffInv = kOffVals1 + up256(kSlots * 4);
 constexpr size_t kOffUf = kOffInv + up256(kSlots * 4);
 constexpr size_t kOffXbits = kOffUf + up256(kPairs * 4);
-constexpr size_t kOffAddr0 = kOffXbits + up256((kPairs / 32 + 1) * 4);
+constexpr size_t kOffYbits = kOffXbits + up256((kPairs / 32 + 1) * 4);
+constexpr size_t kOffAddr0 = kOffYbits + up256((kPairs / 32 + 1) * 4);
 constexpr size_t kOffAddr1 = kOffAddr0 + up256(kNodes * sizeof(NodeAddress));
-constexpr size_t kBytes = kOffAddr1 + up256(kNodes * sizeof(NodeAddress)); // about 4.5 MB
+constexpr size_t kOffOwner = kOffAddr1 + up256(kNodes * sizeof(NodeAddress));
+constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
+constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
+constexpr size_t kOffControl = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
+constexpr size_t kBytes = kOffControl + 256; // about 5.5 MB
 
 } // namespace noalloc
 } // namespace bpb200
@@ -797,8 +929,13 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         w.inv = reinterpret_cast<uint32_t*>(base + noalloc::kOffInv);
         w.uf = reinterpret_cast<uint32_t*>(base + noalloc::kOffUf);
         w.xbits = reinterpret_cast<uint32_t*>(base + noalloc::kOffXbits);
+        w.ybits = reinterpret_cast<uint32_t*>(base + noalloc::kOffYbits);
         w.addr[0] = reinterpret_cast<NodeAddress*>(base + noalloc::kOffAddr0);
         w.addr[1] = reinterpret_cast<NodeAddress*>(base + noalloc::kOffAddr1);
+        w.owner = reinterpret_cast<uint32_t*>(base + noalloc::kOffOwner);
+        w.state[0] = reinterpret_cast<uint4*>(base + noalloc::kOffState0);
+        w.state[1] = reinterpret_cast<uint4*>(base + noalloc::kOffState1);
+        w.control = reinterpret_cast<uint32_t*>(base + noalloc::kOffControl);
         cudaStream_t st = (cudaStream_t)stream;
         // The plan source is ordinary host memory: the copy is staged before
         // cudaMemcpyAsync returns, so g_plan can be reused by the next call.

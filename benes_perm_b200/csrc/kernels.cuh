@@ -4,8 +4,8 @@
 //
 // Level kernels (global memory) run one routing level over every node of
 // the level at once; they are used while nodes are larger than a tile.
-// The tile kernel takes one node per CTA into shared memory and finishes
-// its whole subtree there, down to the middle-group ranks.
+// The tile kernel (tile.cuh) takes one node per CTA into shared memory and
+// finishes its whole subtree there, down to the middle-group ranks.
 //
 // Per internal node and level (src/benes.cpp:226-315):
 //   inverse      inv[p[i]] = i (node-local)
@@ -17,7 +17,12 @@
 //                colouring: each component's smallest vertex gets colour 0);
 //                children left[k] = p[2k+x]/2, right[k] = p[2k+1-x]/2; the
 //                input switch of pair k is x(k)
-//   output bits  output switch of pair k is colour(inv[2k])
+//   ybits        output switch of output pair k is colour(inv[2k])
+//   emit         switch bits into the clustered blob layout, in packet-major
+//                order so a warp's 32 lanes cover consecutive blob bits
+//
+// All loops keep several independent loads per thread in flight: the
+// kernels are bound by memory latency, not by instruction issue.
 #pragma once
 
 #include "device.cuh"
@@ -29,6 +34,9 @@ namespace bpb200 {
 
 constexpr uint32_t kNodeWave = 256;   // node descriptors held in shared memory at once
 constexpr uint32_t kTileThreads = 512;
+constexpr int kInverseItems = 8;      // slots per thread in level_inverse
+constexpr int kUnionItems = 4;        // output pairs per thread in level_union
+constexpr int kResolveItems = 4;      // pair-nodes per thread in level_resolve
 
 struct TileShape {
     uint32_t slots;   // padded entry slots needed at the deepest level
@@ -36,71 +44,262 @@ struct TileShape {
     uint32_t smem;    // dynamic shared memory bytes
 };
 
+// 32-bit node-size test: every level here has fewer than 2^32 nodes.
+__device__ __forceinline__ uint32_t size_at(const LevelInfo& lv, uint32_t level, uint32_t node) {
+    const uint32_t rev = level == 0 ? 0u : (__brev(node) >> (32 - level));
+    return (uint32_t)lv.q + ((uint64_t)rev < lv.r ? 1u : 0u);
+}
+
 // ------------------------------------------------------------ level kernels
 
 template <typename T>
 __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint32_t* __restrict__ inv,
-    uint32_t* __restrict__ uf, uint32_t* status) {
+    uint32_t* __restrict__ uf, uint32_t* __restrict__ owner, uint32_t* claims, uint32_t* status) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t total = (uint64_t)cap << level;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += stride) {
-        const uint32_t j = (uint32_t)(e / cap);
-        const uint32_t i = (uint32_t)(e - (uint64_t)j * cap);
-        const uint32_t s = (uint32_t)node_size(lv, level, j);
-        if (i >= s) {
+    const bool aligned = ((uintptr_t)src & 15u) == 0;
+    uint64_t first;
+    while (claim_chunk(claims, (uint64_t)blockDim.x * kInverseItems, total, &first)) {
+        const uint64_t e0 = first + (uint64_t)threadIdx.x * kInverseItems;
+        if (e0 >= total) {
             continue;
         }
-        const uint64_t v = (uint64_t)src[e];
-        if (v >= s) {
-            atomicOr(status, kErrNotPermutation);
-            continue;
+        T v[kInverseItems];
+        if (aligned && e0 + kInverseItems <= total) {
+            constexpr int kVec = 16 / sizeof(T);
+#pragma unroll
+            for (int q = 0; q < kInverseItems / kVec; ++q) {
+                const uint4 chunk = __ldcs(reinterpret_cast<const uint4*>(src + e0) + q);
+                const T* parts = reinterpret_cast<const T*>(&chunk);
+#pragma unroll
+                for (int r = 0; r < kVec; ++r) v[q * kVec + r] = parts[r];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kInverseItems; ++q) {
+                v[q] = e0 + q < total ? src[e0 + q] : (T)0;
+            }
         }
-        inv[(uint64_t)j * cap + v] = i;
-        if ((i & 1u) == 0) {
-            const uint32_t id = j * pcap + (i >> 1);
-            uf[id] = id << 1;
+        uint32_t j = (uint32_t)(e0 / cap);
+        uint32_t i = (uint32_t)(e0 - (uint64_t)j * cap);
+        uint32_t s = size_at(lv, level, j);
+        // every slot starts unowned for the orbit walks
+        if (e0 + kInverseItems <= total) {
+            uint4* o = reinterpret_cast<uint4*>(owner + e0);
+            o[0] = make_uint4(~0u, ~0u, ~0u, ~0u);
+            o[1] = make_uint4(~0u, ~0u, ~0u, ~0u);
+        } else {
+            for (uint64_t e = e0; e < total; ++e) owner[e] = ~0u;
+        }
+#pragma unroll
+        for (int q = 0; q < kInverseItems; ++q) {
+            if (e0 + q < total && i < s) {
+                const uint64_t val = (uint64_t)v[q];
+                if (val >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                } else {
+                    inv[(uint64_t)j * cap + val] = i;
+                    if ((i & 1u) == 0) {
+                        const uint32_t id = j * pcap + (i >> 1);
+                        uf[id] = id << 1;
+                    }
+                }
+            }
+            if (++i == cap) {
+                i = 0;
+                ++j;
+                s = size_at(lv, level, j);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Partitioned inverse for levels whose nodes do not fit in L2.  A plain
+// scatter inv[p[i]] = i there costs one HBM read-modify-write of a 32-byte
+// sector per entry (about 21 G entries/s on B200).  Instead:
+//   level_bucket  streams the values once and appends (destination, i)
+//                 records to the 2^kPlaceLog2-slot destination window they
+//                 land in (block-local counts in shared memory, one global
+//                 reservation per block and window);
+//   level_place   replays each window's records; the writes of one window
+//                 stay inside an L2-resident 8 MB range.
+// A window receives at most as many records as it has slots when the input
+// is a permutation; an overfull window means a repeated value.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kPlaceLog2 = 21;
+constexpr uint32_t kMaxWindows = 2048;
+constexpr int kBucketItems = 16;
+
+template <typename T>
+__global__ void __launch_bounds__(256) level_bucket(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
+    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
+    __shared__ uint32_t count[kMaxWindows];
+    __shared__ uint32_t start[kMaxWindows];
+    const LevelInfo& lv = plan->levels[level];
+    const uint32_t cap = (uint32_t)lv.cap;
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint64_t total = (uint64_t)cap << level;
+    const uint32_t windows = (uint32_t)((total + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
+    const uint64_t chunk = (uint64_t)blockDim.x * kBucketItems;
+    const bool aligned = ((uintptr_t)src & 15u) == 0;
+    for (uint64_t c0 = (uint64_t)blockIdx.x * chunk; c0 < total; c0 += (uint64_t)gridDim.x * chunk) {
+        for (uint32_t b = threadIdx.x; b < windows; b += blockDim.x) count[b] = 0;
+        __syncthreads();
+        const uint64_t e0 = c0 + (uint64_t)threadIdx.x * kBucketItems;
+        uint32_t dest[kBucketItems], idx[kBucketItems];
+        T v[kBucketItems];
+        if (aligned && e0 + kBucketItems <= total) {
+            constexpr int kVec = 16 / sizeof(T);
+#pragma unroll
+            for (int q = 0; q < kBucketItems / kVec; ++q) {
+                const uint4 part = __ldcs(reinterpret_cast<const uint4*>(src + e0) + q);
+                const T* parts = reinterpret_cast<const T*>(&part);
+#pragma unroll
+                for (int r = 0; r < kVec; ++r) v[q * kVec + r] = parts[r];
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < kBucketItems; ++q) v[q] = e0 + q < total ? src[e0 + q] : (T)0;
+        }
+        uint32_t j = (uint32_t)(e0 < total ? e0 / cap : 0);
+        uint32_t i = (uint32_t)(e0 < total ? e0 - (uint64_t)j * cap : 0);
+        uint32_t s = size_at(lv, level, j);
+#pragma unroll
+        for (int q = 0; q < kBucketItems; ++q) {
+            dest[q] = ~0u;
+            if (e0 + q < total && i < s) {
+                const uint64_t val = (uint64_t)v[q];
+                if (val >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                } else {
+                    dest[q] = j * cap + (uint32_t)val;
+                    idx[q] = i;
+                    atomicAdd(&count[dest[q] >> kPlaceLog2], 1u);
+                    if ((i & 1u) == 0) {
+                        const uint32_t id = j * pcap + (i >> 1);
+                        uf[id] = id << 1;
+                    }
+                }
+            }
+            if (++i == cap) {
+                i = 0;
+                ++j;
+                s = size_at(lv, level, j);
+            }
+        }
+        __syncthreads();
+        for (uint32_t b = threadIdx.x; b < windows; b += blockDim.x) {
+            if (count[b] != 0) start[b] = atomicAdd(cursor + b, count[b]);
+            count[b] = 0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kBucketItems; ++q) {
+            if (dest[q] == ~0u) continue;
+            const uint32_t b = dest[q] >> kPlaceLog2;
+            const uint64_t at = ((uint64_t)b << kPlaceLog2) + start[b] + atomicAdd(&count[b], 1u);
+            if (at < total && at < ((uint64_t)(b + 1) << kPlaceLog2)) {
+                records[at] = make_uint2(dest[q], idx[q]);
+            } else {
+                atomicOr(status, kErrNotPermutation); // more values than slots: a repeat
+            }
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kPlaceItems = 16;
+
+__global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan,
+    uint32_t level, const uint2* __restrict__ records, const uint32_t* __restrict__ cursor,
+    uint32_t* __restrict__ inv, uint32_t* claims) {
+    const LevelInfo& lv = plan->levels[level];
+    const uint64_t total = lv.cap << level;
+    const uint64_t chunk = (uint64_t)blockDim.x * kPlaceItems;
+    uint64_t first;
+    while (claim_chunk(claims, chunk, total, &first)) {
+#pragma unroll
+        for (int q = 0; q < kPlaceItems; ++q) {
+            const uint64_t at = first + (uint64_t)q * blockDim.x + threadIdx.x;
+            if (at >= total) break;
+            const uint32_t b = (uint32_t)(at >> kPlaceLog2);
+            if ((at & ((1ull << kPlaceLog2) - 1)) < cursor[b]) {
+                const uint2 r = __ldcs(records + at);
+                inv[r.x] = r.y;
+            }
         }
     }
 }
 
 __global__ void __launch_bounds__(256) level_union(const Plan* __restrict__ plan,
-    uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, uint32_t* status) {
+    uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard,
+    uint32_t* status) {
+    if (hard != nullptr && *hard == 0) {
+        return; // the orbit walks coloured this level
+    }
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t total = (uint64_t)pcap << level;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < total; p += stride) {
-        const uint32_t j = (uint32_t)(p / pcap);
-        const uint32_t k = (uint32_t)(p - (uint64_t)j * pcap);
-        const uint32_t s = (uint32_t)node_size(lv, level, j);
-        if (k >= s / 2) {
-            continue;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kUnionItems;
+    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kUnionItems;
+         p0 < total; p0 += stride) {
+        uint32_t j = (uint32_t)(p0 / pcap);
+        uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
+        uint32_t s = size_at(lv, level, j);
+        uint32_t a[kUnionItems], b[kUnionItems], rel[kUnionItems];
+        uint32_t u[kUnionItems], w[kUnionItems], base[kUnionItems];
+        uint32_t pending = 0;
+#pragma unroll
+        for (int q = 0; q < kUnionItems; ++q) {
+            if (p0 + q < total && k < s / 2) {
+                pending |= 1u << q;
+                const uint64_t at = (uint64_t)j * cap + 2 * k;
+                u[q] = inv[at];
+                w[q] = inv[at + 1];
+                base[q] = j * pcap;
+                rel[q] = s; // stash the node size for the range check below
+            }
+            if (++k == pcap) {
+                k = 0;
+                ++j;
+                s = size_at(lv, level, j);
+            }
         }
-        const uint32_t u = inv[(uint64_t)j * cap + 2 * k];
-        const uint32_t w = inv[(uint64_t)j * cap + 2 * k + 1];
-        if (u >= s || w >= s) {
-            atomicOr(status, kErrNotPermutation);
-            continue;
+#pragma unroll
+        for (int q = 0; q < kUnionItems; ++q) {
+            if (pending & (1u << q)) {
+                if (u[q] >= rel[q] || w[q] >= rel[q]) {
+                    atomicOr(status, kErrNotPermutation);
+                    pending &= ~(1u << q);
+                    continue;
+                }
+                a[q] = base[q] + (u[q] >> 1);
+                b[q] = base[q] + (w[q] >> 1);
+                rel[q] = 1u ^ (u[q] & 1u) ^ (w[q] & 1u);
+            }
         }
-        const uint32_t base = j * pcap;
-        uf_union(uf, base + (u >> 1), base + (w >> 1), 1u ^ (u & 1u) ^ (w & 1u), status);
+        uf_union_many<kUnionItems>(uf, a, b, rel, pending, status);
     }
 }
 
 __global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
-    const uint32_t* __restrict__ inv, uint32_t* uf, uint32_t* status) {
+    const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard, uint32_t* status) {
+    if (hard != nullptr && *hard == 0) {
+        return;
+    }
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t nodes = 1ull << level;
     for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nodes;
          j += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t s = (uint32_t)node_size(lv, level, j);
+        const uint32_t s = size_at(lv, level, (uint32_t)j);
         if ((s & 1u) == 0) {
             continue;
         }
@@ -125,91 +324,144 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
     }
 }
 
+// Colours of a warp-aligned run of 4*32 pair-nodes, children scatter.
 template <typename T>
 __global__ void __launch_bounds__(256) level_resolve(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint32_t* uf, uint32_t* __restrict__ xbits,
-    uint32_t* __restrict__ dst, const NodeAddress* __restrict__ in_addr,
-    uint32_t* __restrict__ blob, uint32_t* status) {
+    uint32_t* __restrict__ dst, uint32_t* status) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint32_t ccap = (uint32_t)plan->levels[level + 1].cap;
     const uint64_t total = (uint64_t)pcap << level;
-    const uint64_t section_bit = plan->section_offset[0] * 8;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    // Every warp walks whole 32-slot chunks so the ballot covers one word.
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p - (threadIdx.x & 31) < total;
-         p += stride) {
-        const bool in_range = p < total;
-        uint32_t j = 0, k = 0, s = 0;
-        bool live = false;
-        if (in_range) {
-            j = (uint32_t)(p / pcap);
-            k = (uint32_t)(p - (uint64_t)j * pcap);
-            s = (uint32_t)node_size(lv, level, j);
-            live = k < s - s / 2;
-        }
-        uint32_t x = 0;
-        if (live) {
-            const Found f = uf_find(uf, (uint32_t)p, status);
-            x = f.bit ^ (uf_load(uf, f.root) & 1u);
-        }
-        const unsigned word = __ballot_sync(0xffffffffu, x != 0);
-        if ((threadIdx.x & 31) == 0) {
-            xbits[p >> 5] = word;
-        }
-        const uint32_t half = s / 2;
-        if (live) {
-            const uint64_t node = (uint64_t)j * cap;
-            const uint64_t left = (uint64_t)(2 * j) * ccap;
-            const uint64_t right = (uint64_t)(2 * j + 1) * ccap;
-            if (k < half) {
-                const uint32_t a = (uint32_t)src[node + 2 * k + x];
-                const uint32_t b = (uint32_t)src[node + 2 * k + 1 - x];
-                dst[left + k] = a >> 1;
-                dst[right + k] = b >> 1;
-            } else {
-                dst[left + k] = (uint32_t)(src[node + s - 1] >> 1);
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kResolveItems;
+    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kResolveItems;
+         p0 - lane * kResolveItems < total; p0 += stride) {
+        uint32_t j = (uint32_t)(p0 / pcap);
+        uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
+        uint32_t s = size_at(lv, level, j);
+        uint32_t x[kResolveItems], jj[kResolveItems], kk[kResolveItems], ss[kResolveItems];
+        Found f[kResolveItems];
+        uint32_t pending = 0;
+#pragma unroll
+        for (int q = 0; q < kResolveItems; ++q) {
+            x[q] = (uint32_t)(p0 + q);
+            jj[q] = j;
+            kk[q] = k;
+            ss[q] = s;
+            if (p0 + q < total && k < s - s / 2) pending |= 1u << q;
+            if (++k == pcap) {
+                k = 0;
+                ++j;
+                s = size_at(lv, level, j);
             }
         }
-        const bool has_switch = live && k < half;
-        uint64_t bit = 0;
-        if (has_switch) {
-            bit = section_bit + switch_bit(in_addr[j], k);
+        const uint32_t live = pending;
+        uf_find_many<kResolveItems>(uf, x, f, pending, status);
+        uint32_t nibble = 0;
+        uint32_t flag[kResolveItems];
+#pragma unroll
+        for (int q = 0; q < kResolveItems; ++q) {
+            if (live & (1u << q)) flag[q] = uf_load(uf, f[q].root);
         }
-        emit_bit(blob, bit, has_switch && x != 0, 0xffffffffu);
+#pragma unroll
+        for (int q = 0; q < kResolveItems; ++q) {
+            if (!(live & (1u << q))) continue;
+            const uint32_t c = f[q].bit ^ (flag[q] & 1u);
+            nibble |= c << q;
+            const uint64_t node = (uint64_t)jj[q] * cap;
+            const uint64_t left = (uint64_t)(2 * jj[q]) * ccap;
+            const uint64_t right = (uint64_t)(2 * jj[q] + 1) * ccap;
+            const uint32_t half = ss[q] / 2;
+            if (kk[q] < half) {
+                const uint32_t va = (uint32_t)src[node + 2 * kk[q] + c];
+                const uint32_t vb = (uint32_t)src[node + 2 * kk[q] + 1 - c];
+                dst[left + kk[q]] = va >> 1;
+                dst[right + kk[q]] = vb >> 1;
+            } else {
+                dst[left + kk[q]] = (uint32_t)(src[node + ss[q] - 1] >> 1);
+            }
+        }
+        // 8 lanes x 4 bits make one 32-bit word of colour bits
+        uint32_t v = nibble << ((lane & 7) * 4);
+        v |= __shfl_xor_sync(0xffffffffu, v, 1);
+        v |= __shfl_xor_sync(0xffffffffu, v, 2);
+        v |= __shfl_xor_sync(0xffffffffu, v, 4);
+        if ((lane & 7) == 0 && p0 < total) {
+            xbits[p0 >> 5] = v;
+        }
     }
 }
 
-__global__ void __launch_bounds__(256) level_output_bits(const Plan* __restrict__ plan,
+// Output switch bits in natural (node, output pair) order.
+__global__ void __launch_bounds__(256) level_ybits(const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, const uint32_t* __restrict__ xbits,
-    const NodeAddress* __restrict__ out_addr, uint32_t* __restrict__ blob) {
+    uint32_t* __restrict__ ybits) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t total = (uint64_t)pcap << level;
-    const uint64_t section_bit = plan->section_offset[1] * 8;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p - (threadIdx.x & 31) < total;
-         p += stride) {
-        bool has_switch = false;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+         p - (threadIdx.x & 31) < total; p += stride) {
         bool y = false;
-        uint64_t bit = 0;
         if (p < total) {
             const uint32_t j = (uint32_t)(p / pcap);
             const uint32_t k = (uint32_t)(p - (uint64_t)j * pcap);
-            const uint32_t s = (uint32_t)node_size(lv, level, j);
+            const uint32_t s = size_at(lv, level, j);
             if (k < s / 2) {
                 const uint32_t u = inv[(uint64_t)j * cap + 2 * k];
                 if (u < s) {
                     const uint64_t q = (uint64_t)j * pcap + (u >> 1);
                     y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
-                    has_switch = true;
-                    bit = section_bit + switch_bit(out_addr[j], k);
                 }
             }
         }
-        emit_bit(blob, bit, has_switch && y, 0xffffffffu);
+        const unsigned word = __ballot_sync(0xffffffffu, y);
+        if ((threadIdx.x & 31) == 0) {
+            ybits[p >> 5] = word;
+        }
+    }
+}
+
+// Switch bits of one section at one level, packet-major: thread t maps to
+// (packet, node, pair-in-span) with the pair fastest, then the node, so for
+// full packets consecutive threads land on consecutive blob bits and a
+// warp issues one or two atomics instead of one per bit.
+__global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob) {
+    const LevelInfo& lv = plan->levels[level];
+    const LevelSide& ls = lv.side[side];
+    const GroupInfo& gi = plan->groups[side][ls.group];
+    const uint32_t span_log2 = gi.depth - ls.rel - 1;
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint64_t max_pairs = lv.cap / 2;
+    const uint64_t packets = (max_pairs + (1ull << span_log2) - 1) >> span_log2;
+    const uint32_t shift = level + span_log2; // log2(nodes * span)
+    const uint64_t total = packets << shift;
+    const uint64_t section_bit = plan->section_offset[side] * 8;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+         t - (threadIdx.x & 31) < total; t += stride) {
+        bool set = false;
+        uint64_t dest = 0;
+        if (t < total) {
+            const uint64_t packet = t >> shift;
+            const uint64_t rem = t & ((1ull << shift) - 1);
+            const uint32_t node = (uint32_t)(rem >> span_log2);
+            const uint64_t pair = (packet << span_log2) + (rem & ((1ull << span_log2) - 1));
+            const uint32_t s = size_at(lv, level, node);
+            if (pair < s / 2) {
+                const uint64_t q = (uint64_t)node * pcap + pair;
+                set = ((bits[q >> 5] >> (q & 31)) & 1u) != 0;
+                if (set) {
+                    dest = section_bit + switch_bit(addr[node], pair);
+                }
+            }
+        }
+        emit_bit(blob, dest, set, 0xffffffffu);
     }
 }
 

@@ -3,7 +3,7 @@
 // Tile kernel: one CTA per node of the tile level; the node's whole subtree
 // (every remaining routing level plus the middle-group ranks) is encoded in
 // shared memory.  Node-local values fit 16 bits (a tile holds at most a few
-// thousand entries), union-find words are 32-bit smem words.
+// thousand entries), union-find words are 32-bit shared-memory words.
 #pragma once
 
 #include "device.cuh"
@@ -14,51 +14,38 @@
 
 namespace bpb200 {
 
-struct TileSmem {
-    uint16_t* vals[2];
-    uint16_t* inv;
-    uint32_t* uf;
-    uint32_t* xbits;
-    NodeAddress* desc;  // [2][kNodeWave]
-    uint64_t* leafbit;  // [kNodeWave], section in the top 2 bits
-};
-
 __host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
 // Byte offsets of the smem arrays; identical on host (sizing) and device.
 __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pairs,
     uint32_t* off) {
+    const uint32_t words = (pairs + 31) / 32 + 1;
     uint32_t o = 0;
     off[0] = o; o = align_up(o + slots * 2, 16);           // vals[0]
     off[1] = o; o = align_up(o + slots * 2, 16);           // vals[1]
     off[2] = o; o = align_up(o + slots * 2, 16);           // inv
     off[3] = o; o = align_up(o + pairs * 4, 16);           // uf
-    off[4] = o; o = align_up(o + (pairs + 31) / 32 * 4 + 4, 16); // xbits
-    off[5] = o; o = align_up(o + 2 * kNodeWave * (uint32_t)sizeof(NodeAddress), 16);
-    off[6] = o; o = align_up(o + kNodeWave * 8, 16);       // leafbit
+    off[4] = o; o = align_up(o + words * 4, 16);           // xbits (input switches)
+    off[5] = o; o = align_up(o + words * 4, 16);           // ybits (output switches)
+    off[6] = o; o = align_up(o + 2 * kNodeWave * (uint32_t)sizeof(NodeAddress), 16);
+    off[7] = o; o = align_up(o + kNodeWave * 8, 16);       // leafbit
     return o;
 }
 
-__device__ __forceinline__ bool node_exists(const Plan& p, uint32_t level, uint64_t node) {
-    if (level == 0) {
-        return true;
-    }
-    return node_size(p.levels[level - 1], level - 1, node >> 1) > p.leaf;
-}
-
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restrict__ plan_ptr,
+__global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __restrict__ plan_ptr,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
     uint32_t pairs) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t off[7];
+    uint32_t off[8];
     tile_smem_layout(slots, pairs, off);
     uint16_t* vals[2] = {(uint16_t*)(smem + off[0]), (uint16_t*)(smem + off[1])};
     uint16_t* inv = (uint16_t*)(smem + off[2]);
     uint32_t* uf = (uint32_t*)(smem + off[3]);
     uint32_t* xbits = (uint32_t*)(smem + off[4]);
-    NodeAddress* desc = (NodeAddress*)(smem + off[5]);
-    uint64_t* leafbit = (uint64_t*)(smem + off[6]);
+    uint32_t* ybits = (uint32_t*)(smem + off[5]);
+    NodeAddress* desc = (NodeAddress*)(smem + off[6]);
+    uint64_t* leafbit = (uint64_t*)(smem + off[7]);
 
     const Plan& plan = *plan_ptr;
     const uint32_t tid = threadIdx.x;
@@ -68,15 +55,15 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
     const uint32_t T0 = plan.tile_level;
     const uint32_t D = plan.depth;
     const uint32_t leaf = plan.leaf;
-    const uint64_t J = blockIdx.x;
+    const uint32_t J = blockIdx.x;
 
-    if (!node_exists(plan, T0, J)) {
-        return;
+    if (T0 > 0 && size_at(plan.levels[T0 - 1], T0 - 1, J >> 1) <= leaf) {
+        return; // child of a leaf: not part of the tree
     }
     {
         const LevelInfo& l0 = plan.levels[T0];
-        const uint32_t s0 = (uint32_t)node_size(l0, T0, J);
-        const T* in = src + J * l0.cap;
+        const uint32_t s0 = size_at(l0, T0, J);
+        const T* in = src + (uint64_t)J * l0.cap;
         for (uint32_t i = tid; i < s0; i += blockDim.x) {
             const uint64_t v = (uint64_t)in[i];
             if (v >= s0) {
@@ -95,9 +82,17 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
         const uint32_t cap = (uint32_t)lv.cap;
         const uint32_t pcap = (uint32_t)lv.pcap;
         const uint32_t nodes = 1u << t;
-        const uint64_t first = J << t;
+        const uint32_t first = J << t;
         uint16_t* cur = vals[t & 1];
         uint16_t* nxt = vals[(t + 1) & 1];
+        // uniform per level: whether every node here exists / is internal
+        const bool all_exist = level == 0 || plan.levels[level - 1].q > leaf;
+        const bool all_internal = lv.q > leaf && all_exist;
+        auto internal_node = [&](uint32_t path, uint32_t s) {
+            if (all_internal) return true;
+            if (s <= leaf) return false;
+            return all_exist || size_at(plan.levels[level - 1], level - 1, (first + path) >> 1) > leaf;
+        };
 
         if (level < D) {
             if (t == 0 && T0 == 0) {
@@ -112,8 +107,8 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
             for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
                 const uint32_t path = e / cap;
                 const uint32_t i = e - path * cap;
-                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
-                if (i >= s || s <= leaf || !node_exists(plan, level, first + path)) {
+                const uint32_t s = size_at(lv, level, first + path);
+                if (i >= s || !internal_node(path, s)) {
                     continue;
                 }
                 const uint32_t v = cur[e];
@@ -132,8 +127,8 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
             for (uint32_t p = tid; p < nodes * pcap; p += blockDim.x) {
                 const uint32_t path = p / pcap;
                 const uint32_t k = p - path * pcap;
-                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
-                if (s <= leaf || k >= s / 2 || !node_exists(plan, level, first + path)) {
+                const uint32_t s = size_at(lv, level, first + path);
+                if (k >= s / 2 || !internal_node(path, s)) {
                     continue;
                 }
                 const uint32_t u = inv[path * cap + 2 * k];
@@ -148,8 +143,8 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
             __syncthreads();
             // C: orient odd nodes so the unpaired tail gets colour 0
             for (uint32_t path = tid; path < nodes; path += blockDim.x) {
-                const uint32_t s = (uint32_t)node_size(lv, level, first + path);
-                if (s <= leaf || (s & 1u) == 0 || !node_exists(plan, level, first + path)) {
+                const uint32_t s = size_at(lv, level, first + path);
+                if ((s & 1u) == 0 || !internal_node(path, s)) {
                     continue;
                 }
                 if (inv[path * cap + s - 1] >= s) {
@@ -171,8 +166,8 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
                 if (p < ptotal) {
                     const uint32_t path = p / pcap;
                     const uint32_t k = p - path * pcap;
-                    const uint32_t s = (uint32_t)node_size(lv, level, first + path);
-                    if (s > leaf && k < s - s / 2 && node_exists(plan, level, first + path)) {
+                    const uint32_t s = size_at(lv, level, first + path);
+                    if (k < s - s / 2 && internal_node(path, s)) {
                         const Found f = uf_find(uf, p, status);
                         x = f.bit ^ (uf_load(uf, f.root) & 1u);
                         const uint32_t node = path * cap;
@@ -191,46 +186,69 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
                 }
             }
             __syncthreads();
-            // E: switch bits, a wave of node descriptors at a time
-            for (uint32_t w0 = 0; w0 < nodes; w0 += kNodeWave) {
-                const uint32_t wn = nodes - w0 < kNodeWave ? nodes - w0 : kNodeWave;
-                if (tid < 2 * kNodeWave) {
+            // E0: output switch bits in natural order
+            for (uint32_t base = warp * 32; base < ptotal; base += nwarps * 32) {
+                const uint32_t p = base + lane;
+                bool y = false;
+                if (p < ptotal) {
+                    const uint32_t path = p / pcap;
+                    const uint32_t k = p - path * pcap;
+                    const uint32_t s = size_at(lv, level, first + path);
+                    if (k < s / 2 && internal_node(path, s)) {
+                        const uint32_t u = inv[path * cap + 2 * k];
+                        const uint32_t q = path * pcap + (u >> 1);
+                        y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                    }
+                }
+                const unsigned word = __ballot_sync(0xffffffffu, y);
+                if (lane == 0) {
+                    ybits[base >> 5] = word;
+                }
+            }
+            __syncthreads();
+            // E: switch bits, packet-major over a wave of node descriptors
+            const uint32_t wave_log2 = t < 8 ? t : 8; // log2(min(nodes, kNodeWave))
+            const uint32_t wn = 1u << wave_log2;
+            for (uint32_t w0 = 0; w0 < nodes; w0 += wn) {
+                if (tid < 2 * wn) {
                     const uint32_t slot = tid >> 1;
                     const int side = (int)(tid & 1);
-                    if (slot < wn) {
-                        const uint64_t node = first + w0 + slot;
-                        if (node_size(lv, level, node) > leaf && node_exists(plan, level, node)) {
-                            desc[side * kNodeWave + slot] = node_address(plan, side, level, node);
-                        }
+                    const uint32_t node = first + w0 + slot;
+                    const uint32_t s = size_at(lv, level, node);
+                    if (internal_node(w0 + slot, s)) {
+                        desc[side * kNodeWave + slot] = node_address(plan, side, level, node);
                     }
                 }
                 __syncthreads();
-                const uint32_t p0 = w0 * pcap;
-                const uint32_t p1 = (w0 + wn) * pcap;
-                const uint64_t in_bit0 = plan.section_offset[0] * 8;
-                const uint64_t out_bit0 = plan.section_offset[1] * 8;
-                for (uint32_t base = p0 + warp * 32; base < p1; base += nwarps * 32) {
-                    const uint32_t p = base + lane;
-                    bool has = false, xin = false, yout = false;
-                    uint64_t ib = 0, ob = 0;
-                    if (p < p1) {
-                        const uint32_t path = p / pcap;
-                        const uint32_t k = p - path * pcap;
-                        const uint64_t node = first + path;
-                        const uint32_t s = (uint32_t)node_size(lv, level, node);
-                        if (s > leaf && k < s / 2 && node_exists(plan, level, node)) {
-                            has = true;
-                            xin = (xbits[p >> 5] >> (p & 31)) & 1u;
-                            const uint32_t u = inv[path * cap + 2 * k];
-                            const uint32_t q = path * pcap + (u >> 1);
-                            yout = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
-                            const uint32_t slot = path - w0;
-                            ib = in_bit0 + switch_bit(desc[slot], k);
-                            ob = out_bit0 + switch_bit(desc[kNodeWave + slot], k);
+                for (int side = 0; side < 2; ++side) {
+                    const LevelSide& ls = lv.side[side];
+                    const uint32_t span_log2 = plan.groups[side][ls.group].depth - ls.rel - 1;
+                    const uint32_t shift = wave_log2 + span_log2;
+                    const uint32_t packets = (cap / 2 + (1u << span_log2) - 1) >> span_log2;
+                    const uint32_t total = packets << shift;
+                    const uint32_t* bits = side == 0 ? xbits : ybits;
+                    const uint64_t sec = plan.section_offset[side] * 8;
+                    for (uint32_t base = warp * 32; base < total; base += nwarps * 32) {
+                        const uint32_t tt = base + lane;
+                        bool set = false;
+                        uint64_t dest = 0;
+                        if (tt < total) {
+                            const uint32_t packet = tt >> shift;
+                            const uint32_t rem = tt & ((1u << shift) - 1);
+                            const uint32_t slot = rem >> span_log2;
+                            const uint32_t pair = (packet << span_log2) + (rem & ((1u << span_log2) - 1));
+                            const uint32_t path = w0 + slot;
+                            const uint32_t s = size_at(lv, level, first + path);
+                            if (pair < s / 2 && internal_node(path, s)) {
+                                const uint32_t q = path * pcap + pair;
+                                set = ((bits[q >> 5] >> (q & 31)) & 1u) != 0;
+                                if (set) {
+                                    dest = sec + switch_bit(desc[side * kNodeWave + slot], pair);
+                                }
+                            }
                         }
+                        emit_bit(blob, dest, set, 0xffffffffu);
                     }
-                    emit_bit(blob, ib, has && xin, 0xffffffffu);
-                    emit_bit(blob, ob, has && yout, 0xffffffffu);
                 }
                 __syncthreads();
             }
@@ -242,9 +260,11 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
             for (uint32_t w0 = 0; w0 < nodes; w0 += kNodeWave) {
                 const uint32_t wn = nodes - w0 < kNodeWave ? nodes - w0 : kNodeWave;
                 if (tid < wn) {
-                    const uint64_t node = first + w0 + tid;
+                    const uint32_t node = first + w0 + tid;
                     uint64_t v = ~0ull;
-                    if (node_size(lv, level, node) <= leaf && node_exists(plan, level, node)) {
+                    const bool exists = all_exist ||
+                        size_at(plan.levels[level - 1], level - 1, node >> 1) > leaf;
+                    if (size_at(lv, level, node) <= leaf && exists) {
                         int section = 0;
                         const uint64_t bit = leaf_rank_bit(plan, level, node, &section);
                         v = plan.section_offset[section] * 8 + bit;
@@ -258,7 +278,7 @@ __global__ void __launch_bounds__(kTileThreads) tile_encode(const Plan* __restri
                         continue;
                     }
                     const uint32_t path = w0 + li;
-                    const uint32_t s = (uint32_t)node_size(lv, level, first + path);
+                    const uint32_t s = size_at(lv, level, first + path);
                     const uint32_t v = lane < s ? (uint32_t)cur[path * cap + lane] : 0u;
                     if (lane < s && v >= s) {
                         atomicOr(status, kErrNotPermutation);

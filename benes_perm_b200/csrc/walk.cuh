@@ -1,0 +1,418 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// Canonical colouring of the global levels by orbit walks.
+//
+// Within a node of s entries let A(v) = v^1 (input pair partner) and
+// B(u) = inv[p[u]^1] (the input whose output is paired with u's output).
+// The constraint graph (src/benes.cpp:238-252) alternates A and B edges, so
+// each component is a cycle that splits into two orbits of f = B o A,
+// f(v) = inv[p[v^1]^1], mirrors of each other (O and O^1); all vertices of
+// one orbit share a colour and the mirror has the other.  An odd node gets
+// one virtual vertex s with p[s] = s (so inv[s] = s): the reference's tail
+// path then closes into a cycle through s, and giving the tail t = s-1 the
+// smallest key makes "orbit holding the smallest key gets colour 0" exactly
+// the reference's canonical rule (odd tail first, then each component's
+// smallest vertex, src/benes.cpp:253-297):
+//     colour(v) = [min key(O(v)) > min key(O(v^1))],  key(t) = 0, key(v) = v+1.
+//
+// Orbits are long for random inputs, so one vertex in every bucket of
+// 2^kRulerLog2 slots (at a hashed position) is a ruler.  A ruler walks its
+// orbit up to the next ruler, stamping each vertex it passes with its id
+// and keeping the minimum key of the segment and of the segment's mirror.
+// Pointer jumping over rulers (stopping after the first round that changes
+// nothing, which implies convergence on cycles) turns segment minima into
+// orbit minima.  No atomics, no shared roots: every step is two independent
+// gathers.  Cycles without any ruler are short for all but contrived inputs
+// and are walked whole (level_walk_short); a walk longer than kWalkCap sets
+// the `hard` flag and the level falls back to the union-find kernels.
+//
+// Walks pay off while a node's arrays fit in L2 (random access there is
+// 6-8x faster than in HBM on B200); nodes above kWalkMaxNode entries are
+// coloured by union-find, which needs fewer HBM round trips per entry.
+#pragma once
+
+#include "device.cuh"
+#include "kernels.cuh"
+#include "plan.hpp"
+
+#include <cstdint>
+
+namespace bpb200 {
+
+constexpr uint32_t kRulerLog2 = 5;           // one ruler per 32 slots
+constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
+constexpr uint32_t kWalkChunk = 16;          // rulers claimed per warp at a time
+constexpr uint64_t kWalkMaxNode = 1ull << 22; // larger nodes are coloured by union-find
+constexpr uint32_t kUnset = 0xffffffffu;     // owner of a vertex no walk reached
+constexpr uint32_t kColourTag = 0x80000000u; // owner value carrying a colour directly
+constexpr uint32_t kNoRuler = 0xffffffffu;   // bucket whose hashed slot is padding
+
+// control words of a level
+enum : int {
+    kCtlHard = 0,
+    kCtlChanged = 1,
+    kCtlDone = 2,
+    kCtlFinal = 3,
+    kCtlClaim = 4,       // ruler chunks handed out by level_walk
+    kCtlClaimPlace = 5,  // chunks handed out by level_place
+    kCtlClaimInverse = 6, // chunks handed out by level_inverse
+    kCtlWords = 8
+};
+
+__device__ __forceinline__ uint32_t ruler_position(uint32_t bucket) {
+    return (bucket * 0x9E3779B1u) >> (32 - kRulerLog2);
+}
+
+__device__ __forceinline__ bool is_ruler_slot(uint32_t slot) {
+    return (slot & ((1u << kRulerLog2) - 1)) == ruler_position(slot >> kRulerLog2);
+}
+
+// One node of one level, as seen by a walker.
+template <typename T>
+struct NodeView {
+    const T* p;            // node's values (node-local)
+    const uint32_t* inv;   // node's inverse
+    uint32_t s;            // entries
+    bool odd;
+
+    // f(v) = inv[p[v^1]^1] with the virtual vertex s of an odd node; returns
+    // 0xffffffff when a value is out of range (input is not a permutation)
+    __device__ __forceinline__ uint32_t f(uint32_t v) const {
+        const uint32_t a = v ^ 1u;
+        uint32_t o;
+        if (odd && a == s) {
+            o = s;
+        } else {
+            const uint64_t value = (uint64_t)p[a];
+            if (value >= s) {
+                return 0xffffffffu;
+            }
+            o = (uint32_t)value;
+        }
+        const uint32_t b = o ^ 1u;
+        return (odd && b == s) ? s : inv[b];
+    }
+    __device__ __forceinline__ uint32_t key(uint32_t v) const {
+        return (odd && v == s - 1) ? 0u : v + 1;
+    }
+};
+
+// Ruler walks.  Warps claim chunks of kWalkChunk rulers in address order
+// from a per-level counter, so the walks in flight at any moment touch a
+// window of a few tens of MB that stays in L2; within a warp each lane takes
+// the next ruler of the chunk as soon as its current walk ends, so walk
+// lengths (geometric, mean 2^kRulerLog2) do not leave lanes idle behind the
+// longest walk.  state[r] = {next ruler, min key, min mirror key, 0};
+// owner[slot] = r for every real vertex the walk passes.
+template <typename T>
+__global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan, uint32_t level,
+    const T* __restrict__ vals, const uint32_t* __restrict__ inv, uint32_t* __restrict__ owner,
+    uint4* __restrict__ state, uint32_t* control) {
+    const LevelInfo& lv = plan->levels[level];
+    const uint32_t cap = (uint32_t)lv.cap;
+    const uint64_t total = (uint64_t)cap << level;
+    const uint32_t buckets = (uint32_t)((total + (1u << kRulerLog2) - 1) >> kRulerLog2);
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    uint32_t next_free = 0, hi = 0; // current chunk, warp-uniform
+    bool exhausted = false;
+    bool active = false;
+    uint32_t r = 0, base = 0, s = 0, cur = 0, ma = 0, mb = 0, steps = 0;
+    bool odd = false;
+    for (;;) {
+        const unsigned idle = __ballot_sync(0xffffffffu, !active);
+        if (idle != 0 && next_free >= hi && !exhausted) {
+            uint32_t c = 0;
+            if (lane == 0) c = atomicAdd(control + kCtlClaim, 1u);
+            c = __shfl_sync(0xffffffffu, c, 0);
+            const uint64_t lo = (uint64_t)c * kWalkChunk;
+            if (lo >= buckets) {
+                exhausted = true;
+            } else {
+                next_free = (uint32_t)lo;
+                hi = (uint32_t)(lo + kWalkChunk < buckets ? lo + kWalkChunk : buckets);
+            }
+        }
+        if (!active) {
+            const uint32_t mine = next_free + (uint32_t)__popc(idle & below);
+            if (mine < hi) {
+                r = mine;
+                const uint32_t slot = (r << kRulerLog2) + ruler_position(r);
+                const uint32_t j = slot < total ? slot / cap : 0u;
+                const uint32_t v0 = slot - j * cap;
+                s = slot < total ? size_at(lv, level, j) : 0u;
+                if (slot >= total || v0 >= s) {
+                    state[r] = make_uint4(kNoRuler, 0, 0, 0);
+                } else {
+                    base = j * cap;
+                    odd = (s & 1u) != 0;
+                    const NodeView<T> nv{vals + base, inv + base, s, odd};
+                    cur = v0;
+                    ma = nv.key(v0);
+                    mb = nv.key(v0 ^ 1u);
+                    steps = 0;
+                    active = true;
+                }
+            }
+        }
+        next_free = min(next_free + (uint32_t)__popc(idle), hi);
+        if (__ballot_sync(0xffffffffu, active) == 0) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active) {
+            const NodeView<T> nv{vals + base, inv + base, s, odd};
+            const uint32_t w = nv.f(cur);
+            bool end = false;
+            uint32_t next = r;
+            if (w >= s + (odd ? 1u : 0u)) {
+                atomicOr(control + kCtlHard, 1u); // not a permutation
+                end = true;
+            } else if (w < s && is_ruler_slot(base + w)) {
+                next = (base + w) >> kRulerLog2;
+                end = true;
+            } else {
+                if (w < s) owner[base + w] = r;
+                ma = min(ma, nv.key(w));
+                mb = min(mb, nv.key(w ^ 1u));
+                cur = w;
+                if (++steps == kWalkCap) {
+                    atomicOr(control + kCtlHard, 1u);
+                    end = true;
+                }
+            }
+            if (end) {
+                state[r] = make_uint4(next, ma, mb, 0);
+                active = false;
+            }
+        }
+    }
+}
+
+// Cycles no ruler reached (both orbits ruler-free): thread per pair-node
+// whose two vertices are unowned.  Only the walker starting at the smallest
+// even vertex of its orbit walks the orbit whole (the others stop at the
+// first smaller even vertex, about log L steps), then stamps the orbit's
+// colour on every real vertex of it.  Every even vertex of the cycle lies in
+// one of the two orbits, so every pair-node of the cycle gets a stamped
+// colour; the cost is O(L log L) per cycle.
+template <typename T>
+__global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ vals, const uint32_t* __restrict__ inv,
+    uint32_t* __restrict__ owner, uint32_t* control) {
+    const LevelInfo& lv = plan->levels[level];
+    const uint32_t cap = (uint32_t)lv.cap;
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint64_t total = (uint64_t)pcap << level;
+    for (uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pidx < total;
+         pidx += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t j = (uint32_t)(pidx / pcap);
+        const uint32_t k = (uint32_t)(pidx - (uint64_t)j * pcap);
+        const uint32_t s = size_at(lv, level, j);
+        if (k >= s - s / 2) {
+            continue;
+        }
+        const uint32_t base = j * cap;
+        const uint32_t v = 2 * k;
+        if (is_ruler_slot(base + v) || owner[base + v] != kUnset) {
+            continue;
+        }
+        if (v + 1 < s && (is_ruler_slot(base + v + 1) || owner[base + v + 1] != kUnset)) {
+            continue;
+        }
+        const NodeView<T> nv{vals + base, inv + base, s, (s & 1u) != 0};
+        const uint32_t mine = nv.key(v);
+        uint32_t ma = mine, mb = nv.key(v ^ 1u);
+        uint32_t cur = v;
+        bool closed = false, smallest = true;
+        for (uint32_t step = 0; step < kWalkCap; ++step) {
+            const uint32_t w = nv.f(cur);
+            if (w >= s + (nv.odd ? 1u : 0u)) {
+                break;
+            }
+            if (w == v) {
+                closed = true;
+                break;
+            }
+            if ((w & 1u) == 0 && w < s && nv.key(w) < mine) {
+                smallest = false; // that vertex's walker covers this orbit
+                closed = true;
+                break;
+            }
+            ma = min(ma, nv.key(w));
+            mb = min(mb, nv.key(w ^ 1u));
+            cur = w;
+        }
+        if (!closed) {
+            atomicOr(control + kCtlHard, 1u);
+            continue;
+        }
+        if (!smallest) {
+            continue;
+        }
+        const uint32_t colour = kColourTag | (ma > mb ? 1u : 0u);
+        cur = v;
+        do {
+            if (cur < s) owner[base + cur] = colour;
+            cur = nv.f(cur);
+        } while (cur != v);
+    }
+}
+
+// One pointer-jumping round over ruler states (src -> dst).
+__global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
+    uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
+    if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
+        *(volatile uint32_t*)(control + kCtlHard) != 0) {
+        return;
+    }
+    bool changed = false;
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rulers;
+         r += gridDim.x * blockDim.x) {
+        const uint4 me = src[r];
+        if (me.x == kNoRuler) {
+            dst[r] = me;
+            continue;
+        }
+        const uint4 nx = src[me.x];
+        const uint4 out = make_uint4(nx.x, min(me.y, nx.y), min(me.z, nx.z), 0);
+        changed |= (out.y != me.y) || (out.z != me.z);
+        dst[r] = out;
+    }
+    if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) {
+        atomicOr(control + kCtlChanged, 1u);
+    }
+    (void)round;
+}
+
+// After a round: a round that changed nothing means every ruler holds its
+// orbit's minima; later rounds then return at once.
+__global__ void ruler_check(uint32_t round, uint32_t* control) {
+    if (control[kCtlDone] != 0 || control[kCtlHard] != 0) {
+        return;
+    }
+    control[kCtlFinal] = (round + 1) & 1u; // buffer the round just wrote
+    if (control[kCtlChanged] == 0) {
+        control[kCtlDone] = 1;
+    }
+    control[kCtlChanged] = 0;
+}
+
+// Clears the level's control words; `force_union_find` pre-sets the hard
+// flag so the level is coloured by union-find (a test hook for that path).
+__global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
+    if (threadIdx.x < kCtlWords) {
+        control[threadIdx.x] = threadIdx.x == kCtlHard ? force_union_find : 0u;
+    }
+}
+
+// Colours (from the walks, or from union-find when the level fell back),
+// children and the colour bitmap: thread per 4 pair-nodes.
+template <typename T>
+__global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
+    const uint4* __restrict__ state0, const uint4* __restrict__ state1, uint32_t* uf,
+    uint32_t* __restrict__ xbits, uint32_t* __restrict__ dst, const uint32_t* control,
+    uint32_t* status) {
+    const LevelInfo& lv = plan->levels[level];
+    const uint32_t cap = (uint32_t)lv.cap;
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint32_t ccap = (uint32_t)plan->levels[level + 1].cap;
+    const uint64_t total = (uint64_t)pcap << level;
+    const bool hard = control[kCtlHard] != 0;
+    const uint4* state = control[kCtlFinal] ? state1 : state0;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kResolveItems;
+    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kResolveItems;
+         p0 - lane * kResolveItems < total; p0 += stride) {
+        uint32_t j = (uint32_t)(p0 / pcap);
+        uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
+        uint32_t s = size_at(lv, level, j);
+        uint32_t jj[kResolveItems], kk[kResolveItems], ss[kResolveItems], c[kResolveItems];
+        uint32_t live = 0;
+#pragma unroll
+        for (int q = 0; q < kResolveItems; ++q) {
+            jj[q] = j;
+            kk[q] = k;
+            ss[q] = s;
+            c[q] = 0;
+            if (p0 + q < total && k < s - s / 2) live |= 1u << q;
+            if (++k == pcap) {
+                k = 0;
+                ++j;
+                s = size_at(lv, level, j);
+            }
+        }
+        if (hard) {
+            uint32_t x[kResolveItems];
+            Found f[kResolveItems];
+#pragma unroll
+            for (int q = 0; q < kResolveItems; ++q) x[q] = (uint32_t)(p0 + q);
+            uf_find_many<kResolveItems>(uf, x, f, live, status);
+#pragma unroll
+            for (int q = 0; q < kResolveItems; ++q) {
+                if (live & (1u << q)) c[q] = f[q].bit ^ (uf_load(uf, f[q].root) & 1u);
+            }
+        } else {
+            // ruler id (or direct colour) of vertex 2k, else of 2k+1
+            uint32_t id[kResolveItems], flip[kResolveItems];
+#pragma unroll
+            for (int q = 0; q < kResolveItems; ++q) {
+                if (!(live & (1u << q))) continue;
+                const uint32_t slot = jj[q] * cap + 2 * kk[q];
+                flip[q] = 0;
+                if (is_ruler_slot(slot)) {
+                    id[q] = slot >> kRulerLog2;
+                } else {
+                    id[q] = owner[slot];
+                    if (id[q] == kUnset && 2 * kk[q] + 1 < ss[q]) {
+                        flip[q] = 1;
+                        id[q] = is_ruler_slot(slot + 1) ? (slot + 1) >> kRulerLog2 : owner[slot + 1];
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kResolveItems; ++q) {
+                if (!(live & (1u << q))) continue;
+                uint32_t colour;
+                if (id[q] == kUnset) {
+                    atomicOr(status, kErrInconsistent); // a walk must have reached it
+                    colour = 0;
+                } else if (id[q] & kColourTag) {
+                    colour = id[q] & 1u;
+                } else {
+                    const uint4 st = state[id[q]];
+                    colour = st.y > st.z ? 1u : 0u;
+                }
+                c[q] = colour ^ flip[q];
+            }
+        }
+        uint32_t nibble = 0;
+#pragma unroll
+        for (int q = 0; q < kResolveItems; ++q) {
+            if (!(live & (1u << q))) continue;
+            nibble |= c[q] << q;
+            const uint64_t node = (uint64_t)jj[q] * cap;
+            const uint64_t left = (uint64_t)(2 * jj[q]) * ccap;
+            const uint64_t right = (uint64_t)(2 * jj[q] + 1) * ccap;
+            const uint32_t half = ss[q] / 2;
+            if (kk[q] < half) {
+                const uint32_t va = (uint32_t)src[node + 2 * kk[q] + c[q]];
+                const uint32_t vb = (uint32_t)src[node + 2 * kk[q] + 1 - c[q]];
+                dst[left + kk[q]] = va >> 1;
+                dst[right + kk[q]] = vb >> 1;
+            } else {
+                dst[left + kk[q]] = (uint32_t)(src[node + ss[q] - 1] >> 1);
+            }
+        }
+        uint32_t v = nibble << ((lane & 7) * 4);
+        v |= __shfl_xor_sync(0xffffffffu, v, 1);
+        v |= __shfl_xor_sync(0xffffffffu, v, 2);
+        v |= __shfl_xor_sync(0xffffffffu, v, 4);
+        if ((lane & 7) == 0 && p0 < total) {
+            xbits[p0 >> 5] = v;
+        }
+    }
+}
+
+} // namespace bpb200

@@ -83,7 +83,7 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
  * allocation can imply.  Same arguments and result bytes as
  * bpb200_compress_device (device input and blob, work queued on `stream`),
  * but every byte of scratch comes from one fixed device array inside this
- * library (about 4.5 MB, present on every GPU that loads the library until
+ * library (about 5.5 MB, present on every GPU that loads the library until
  * the process exits), so it accepts at most 262144 (2^18) entries and
  * returns BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.
  * The first call on each device looks up the array's device address
@@ -113,9 +113,14 @@ void bpb200_shutdown(void);
  * of later calls is bracketed by CUDA events.  bpb200_last_profile reports,
  * for the calling thread's last call, seconds and launch counts per kernel
  * kind (0 prologue, 1 inverse, 2 descriptors, 3 union, 4 orient, 5 resolve,
- * 6 output bits, 7 tile) and the total number of kernel launches; it returns
+ * 6 output bits, 7 tile, 8 emit) and the total number of kernel launches; it returns
  * the number of kinds. */
 void bpb200_set_profiling(int enabled);
+
+/* Test hook: nonzero makes later calls colour every global level with the
+ * union-find kernels instead of the orbit walks (the path the walks fall
+ * back to on contrived inputs).  Output bytes are identical either way. */
+void bpb200_set_colouring(int union_find_only);
 
 /* Geometry of the encode the library would run for (count, format): the
  * routing depth and the first level handled by the shared-memory tile
@@ -124,6 +129,11 @@ int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth
     uint32_t* tile_level);
 int bpb200_last_profile(double* seconds, uint32_t* launches, int kinds,
     uint32_t* total_launches);
+
+/* Per-launch detail of the same profile: kernel kind, routing level and
+ * seconds of each timed launch, in launch order (up to `capacity`); returns
+ * the number of timed launches of the last call. */
+int bpb200_last_profile_launches(int* kinds, int* levels, double* seconds, int capacity);
 
 /* Address probes of the closed-form layout (test hooks, no device work):
  * section-relative bit of switch `pair` of node `node` at routing level

@@ -94,6 +94,34 @@ def test_format_options(gpu, oracle):
                     assert got == oracle.compress(perm, oracle_format(kw)), (n, kw)
 
 
+@pytest.mark.parametrize("union_find_only", [False, True])
+def test_global_levels_both_colourings(gpu, oracle, union_find_only):
+    # sizes that run several global levels (nodes above 8192 entries)
+    gpu.set_union_find_only(union_find_only)
+    try:
+        for n, kind in ((40000, 0), (65537, 1), (131072, 4), (100003, 2), (99999, 3)):
+            perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0x600D + n, n)
+            for kw in (dict(), dict(middle_group_log2=3, middle_placement=1)):
+                got = gpu.compress(perm, gpu.CompressOptions(format=b200_format(gpu, kw)))
+                assert got == oracle.compress(perm, oracle_format(kw)), (n, kind, kw)
+    finally:
+        gpu.set_union_find_only(False)
+
+
+def test_partitioned_inverse_levels(gpu, oracle):
+    # nodes above 2^22 entries take the partitioned inverse and union-find
+    n = (1 << 22) + 4097
+    for kind, dtype in ((0, np.uint32), (1, np.uint64)):
+        perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0xB1C + kind, n, dtype)
+        kw = dict(middle_group_log2=4, middle_placement=2)
+        got = gpu.compress(perm, gpu.CompressOptions(format=b200_format(gpu, kw)))
+        assert got == oracle.compress(perm, oracle_format(kw)), kind
+    bad = gpu.fill_permutation(gpu.PermutationKind.uniform, 5, n)
+    bad[n // 3] = bad[n // 2]
+    with pytest.raises(ValueError):
+        gpu.compress(bad)
+
+
 def test_invalid_inputs_then_recovery(gpu, oracle):
     for bad in ([0, 1, 1], [0, 1, 3], [5, 0, 1, 2, 3, 4, 4]):
         for dt in (np.uint32, np.uint64):

@@ -49,6 +49,11 @@ def parse_args():
     ap.add_argument("--log2n", type=int, default=30, help="workload size (default 30)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="headline", choices=("headline", "serving"),
+                    help="serving: the mixed-size request stream (not the headline metric)")
+    ap.add_argument("--requests", type=int, default=1024, help="serving: number of requests")
+    ap.add_argument("--max-log2", type=int, default=24, help="serving: largest log2 N")
+    ap.add_argument("--hbm-budget", type=int, default=120 * 10**9, help="serving: admission budget")
     return ap.parse_args()
 
 
@@ -369,9 +374,97 @@ def _section_bits(n, fmt):
     return sizes(n)
 
 
+def serving_arm(args):
+    """Mixed-size request stream: plain per-request calls, then the serving
+    loop with Poisson arrivals at 1.5x the plain path's request rate."""
+    import concurrent.futures as futures
+    import hashlib
+    import threading
+
+    import benes_perm_b200 as bp
+
+    rng = np.random.default_rng(SEED)
+    specs = []
+    for i in range(args.requests):
+        n = int(round(2 ** rng.uniform(10, args.max_log2)))
+        kind = int(rng.integers(0, 2))                   # Fisher-Yates or Sattolo
+        dtype = np.uint32 if rng.integers(0, 2) == 0 else np.uint64
+        m = int(rng.choice([4, 5]))
+        placement = int(rng.integers(0, 3))
+        specs.append((n, kind, dtype, m, placement))
+    opts = [bp.CompressOptions(format=bp.FormatOptions(middle_group_log2=m,
+                                                       middle_placement=bp.MiddlePlacement(pl)))
+            for (_, _, _, m, pl) in specs]
+
+    def make(i):
+        n, kind, dtype, _, _ = specs[i]
+        return bp.fill_permutation(bp.PermutationKind(kind), SEED + i, n, dtype)
+
+    with futures.ThreadPoolExecutor(16) as pool:
+        perms = list(pool.map(make, range(len(specs))))
+    total = sum(p.size for p in perms)
+    for p, o in zip(perms[:8], opts[:8]):                # warm-up
+        bp.compress(p, o)
+
+    t0 = time.perf_counter()
+    plain = [hashlib.sha256(bp.compress(p, o)).digest() for p, o in zip(perms, opts)]
+    t_plain = time.perf_counter() - t0
+    plain_rate = total / t_plain
+
+    rate = 1.5 * len(perms) / t_plain                    # offered load, requests/s
+    gaps = rng.exponential(1.0 / rate, len(perms))
+    arrivals = np.cumsum(gaps)
+    server = bp.Server(hbm_budget_bytes=args.hbm_budget, max_batch=256, workers=4)
+    tickets = [None] * len(perms)
+    ready = [threading.Event() for _ in perms]
+
+    def submitter():
+        start = time.perf_counter()
+        for i, (p, o) in enumerate(zip(perms, opts)):
+            delay = arrivals[i] - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            tickets[i] = server.submit(p, o)
+            ready[i].set()
+
+    t1 = time.perf_counter()
+    th = threading.Thread(target=submitter)
+    th.start()
+    identical = True
+    latencies = []
+    for i in range(len(perms)):
+        ready[i].wait()
+        blob, lat = server.wait(tickets[i])
+        latencies.append(lat)
+        identical &= hashlib.sha256(blob).digest() == plain[i]
+    t_serve = time.perf_counter() - t1
+    th.join()
+    stats = server.stats()
+    server.close()
+    lat = np.sort(np.array(latencies))
+    line = {
+        "metric": "entries/s on the mixed-size serving stream (serving loop vs plain per-request)",
+        "value": total / t_serve, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
+        "plain_per_request": plain_rate, "ratio_vs_plain": (total / t_serve) / plain_rate,
+        "p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+        "offered_load_requests_per_s": rate, "identical_bytes": bool(identical),
+        "kernel_launches": stats["kernel_launches"], "data": "synthetic",
+        "config": {"workload": f"{len(perms)} requests, N = round(2^U(10,{args.max_log2})), "
+                               "Fisher-Yates or Sattolo, uint32 or uint64, m in {4,5}, "
+                               "placement uniform over 3, default clusters, Poisson arrivals",
+                   "entries": int(total), "hbm_budget_bytes": args.hbm_budget,
+                   "timing": "host wall clock (submit to blob in host memory)"},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args.gpus)
+    if args.workload == "serving":
+        if rank == 0:
+            serving_arm(args)
+        return
     if args.impl == "reference":
         reference_arm(args, world, rank)
     else:

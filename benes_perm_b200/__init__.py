@@ -287,6 +287,123 @@ def compress_device(d_entries: int, count: int, entry_bytes: int, d_blob: int, b
     return secs.value
 
 
+class _Request(ctypes.Structure):
+    _fields_ = [
+        ("d_entries", ctypes.c_void_p),
+        ("count", ctypes.c_uint64),
+        ("entry_bytes", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("format", _Format),
+        ("d_blob", ctypes.c_void_p),
+        ("blob_len", ctypes.c_uint64),
+        ("status", ctypes.c_int),
+        ("error", ctypes.c_char * 124),
+    ]
+
+
+def compress_batch_device(items, stream: int = 0):
+    """Batched form: ``items`` is a list of
+    (d_entries, count, entry_bytes, FormatOptions, d_blob, blob_len) with
+    device pointers.  Returns (statuses, kernel launches); raises for the
+    first failing request."""
+    lib = library()
+    arr = (_Request * len(items))()
+    for i, (d_in, n, width, fmt, d_blob, blob_len) in enumerate(items):
+        arr[i].d_entries = d_in
+        arr[i].count = n
+        arr[i].entry_bytes = width
+        arr[i].format = to_c_format(fmt)
+        arr[i].d_blob = d_blob
+        arr[i].blob_len = blob_len
+    launches = ctypes.c_uint32(0)
+    lib.bpb200_compress_batch.argtypes = [ctypes.POINTER(_Request), ctypes.c_uint32,
+                                          ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]
+    rc = lib.bpb200_compress_batch(arr, len(items), stream, ctypes.byref(launches))
+    statuses = [arr[i].status for i in range(len(items))]
+    if rc != 0:
+        bad = next(i for i, s in enumerate(statuses) if s != 0)
+        raise_for(statuses[bad], arr[bad].error.decode())
+    return statuses, launches.value
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("submitted", "completed", "failed", "entries", "kernel_launches")] + \
+               [(n, ctypes.c_double) for n in ("p50_seconds", "p99_seconds", "mean_seconds")]
+
+
+class Server:
+    """Serving form: a request loop with HBM-budget admission and continuous
+    batching (bpb200_server_*).  ``submit`` returns a ticket; ``wait`` returns
+    (blob bytes, latency seconds) and raises like ``compress`` on failure."""
+
+    def __init__(self, hbm_budget_bytes: int = 120 * 10**9, max_batch: int = 256,
+                 workers: int = 4):
+        lib = library()
+        lib.bpb200_server_create.restype = ctypes.c_void_p
+        lib.bpb200_server_create.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                             ctypes.c_char_p, ctypes.c_size_t]
+        lib.bpb200_server_submit.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64,
+                                             ctypes.c_uint32, ctypes.POINTER(_Format),
+                                             ctypes.c_void_p, ctypes.c_uint64,
+                                             ctypes.POINTER(ctypes.c_uint64)]
+        lib.bpb200_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_double), ctypes.c_char_p,
+                                           ctypes.c_size_t]
+        lib.bpb200_server_get_stats.argtypes = [ctypes.c_void_p, ctypes.POINTER(_ServerStats)]
+        lib.bpb200_server_destroy.argtypes = [ctypes.c_void_p]
+        lib.bpb200_server_destroy.restype = None
+        err = ctypes.create_string_buffer(256)
+        self._lib = lib
+        self._handle = lib.bpb200_server_create(int(hbm_budget_bytes), max_batch, workers, err, 256)
+        if not self._handle:
+            raise RuntimeError(err.value.decode() or "server creation failed")
+        self._held = {}
+
+    def submit(self, permutation, options: Optional[CompressOptions] = None) -> int:
+        options = options or CompressOptions()
+        arr = np.ascontiguousarray(permutation)
+        if arr.dtype not in (np.uint32, np.uint64):
+            raise TypeError("permutation must be uint32 or uint64")
+        n = int(arr.size)
+        if n == 0:
+            raise ValueError("permutation size is out of range")
+        size = encoded_size(n, options.format)
+        blob = np.empty(size, dtype=np.uint8)
+        cf = to_c_format(options.format)
+        ticket = ctypes.c_uint64(0)
+        rc = self._lib.bpb200_server_submit(self._handle, arr.ctypes.data, n, arr.dtype.itemsize,
+                                            ctypes.byref(cf), blob.ctypes.data, size,
+                                            ctypes.byref(ticket))
+        raise_for(rc, "submit failed")
+        self._held[ticket.value] = (arr, blob, cf)
+        return ticket.value
+
+    def wait(self, ticket: int):
+        err = ctypes.create_string_buffer(256)
+        latency = ctypes.c_double(0)
+        rc = self._lib.bpb200_server_wait(self._handle, ticket, ctypes.byref(latency), err, 256)
+        _, blob, _ = self._held.pop(ticket, (None, None, None))
+        raise_for(rc, err.value.decode())
+        return blob.tobytes(), latency.value
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        self._lib.bpb200_server_get_stats(self._handle, ctypes.byref(s))
+        return {n: getattr(s, n) for n, _ in _ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._handle:
+            self._lib.bpb200_server_destroy(self._handle)
+            self._handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def fill_permutation(kind: PermutationKind, seed: int, count: int,
                      dtype=np.uint32, out: Optional[np.ndarray] = None) -> np.ndarray:
     """Seeded synthetic permutation (xoshiro256** from splitmix64(seed))."""

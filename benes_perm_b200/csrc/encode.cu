@@ -590,15 +590,25 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     return kOk;
 }
 
+// Whether the current device is an sm_100 part, cached per device: the
+// check runs on every call, and a full cudaGetDeviceProperties costs
+// milliseconds.
 int current_device_ok(int* device) {
-    if (cudaGetDevice(device) != cudaSuccess) {
+    static std::atomic<int> known[64]; // 0 unknown, 1 usable, 2 not usable
+    if (cudaGetDevice(device) != cudaSuccess || *device < 0) {
         return 0;
     }
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, *device) != cudaSuccess) {
+    if (*device < 64) {
+        const int k = known[*device].load();
+        if (k != 0) return k == 1 ? 1 : 0;
+    }
+    int major = 0;
+    if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, *device) != cudaSuccess) {
         return 0;
     }
-    return prop.major == 10 ? 1 : 0;
+    const int ok = major == 10 ? 1 : 0;
+    if (*device < 64) known[*device].store(ok ? 1 : 2);
+    return ok;
 }
 
 template <typename Fn>
@@ -972,3 +982,6 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         return kOk;
     });
 }
+
+// Batched and serving forms (share this file's pool, planning and launches).
+#include "serve.inc"

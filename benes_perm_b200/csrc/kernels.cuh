@@ -97,15 +97,17 @@ __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ pl
 #pragma unroll
         for (int q = 0; q < kInverseItems; ++q) {
             if (e0 + q < total && i < s) {
+                // every pair-node starts as its own root, whatever its values:
+                // a stale word could point outside the array
+                if ((i & 1u) == 0) {
+                    const uint32_t id = j * pcap + (i >> 1);
+                    uf[id] = id << 1;
+                }
                 const uint64_t val = (uint64_t)v[q];
                 if (val >= s) {
                     atomicOr(status, kErrNotPermutation);
                 } else {
                     inv[(uint64_t)j * cap + val] = i;
-                    if ((i & 1u) == 0) {
-                        const uint32_t id = j * pcap + (i >> 1);
-                        uf[id] = id << 1;
-                    }
                 }
             }
             if (++i == cap) {
@@ -173,6 +175,10 @@ __global__ void __launch_bounds__(256) level_bucket(const Plan* __restrict__ pla
         for (int q = 0; q < kBucketItems; ++q) {
             dest[q] = ~0u;
             if (e0 + q < total && i < s) {
+                if ((i & 1u) == 0) { // unconditional: see level_inverse
+                    const uint32_t id = j * pcap + (i >> 1);
+                    uf[id] = id << 1;
+                }
                 const uint64_t val = (uint64_t)v[q];
                 if (val >= s) {
                     atomicOr(status, kErrNotPermutation);
@@ -180,10 +186,6 @@ __global__ void __launch_bounds__(256) level_bucket(const Plan* __restrict__ pla
                     dest[q] = j * cap + (uint32_t)val;
                     idx[q] = i;
                     atomicAdd(&count[dest[q] >> kPlaceLog2], 1u);
-                    if ((i & 1u) == 0) {
-                        const uint32_t id = j * pcap + (i >> 1);
-                        uf[id] = id << 1;
-                    }
                 }
             }
             if (++i == cap) {

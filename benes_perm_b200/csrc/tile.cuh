@@ -33,10 +33,9 @@ __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pa
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __restrict__ plan_ptr,
+__device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
-    uint32_t pairs) {
-    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t pairs, uint32_t tile, unsigned char* smem) {
     uint32_t off[8];
     tile_smem_layout(slots, pairs, off);
     uint16_t* vals[2] = {(uint16_t*)(smem + off[0]), (uint16_t*)(smem + off[1])};
@@ -55,7 +54,7 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
     const uint32_t T0 = plan.tile_level;
     const uint32_t D = plan.depth;
     const uint32_t leaf = plan.leaf;
-    const uint32_t J = blockIdx.x;
+    const uint32_t J = tile;
 
     if (T0 > 0 && size_at(plan.levels[T0 - 1], T0 - 1, J >> 1) <= leaf) {
         return; // child of a leaf: not part of the tree
@@ -111,16 +110,16 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
                 if (i >= s || !internal_node(path, s)) {
                     continue;
                 }
+                if ((i & 1u) == 0) { // every pair-node is a root, whatever its values
+                    const uint32_t id = path * pcap + (i >> 1);
+                    uf[id] = id << 1;
+                }
                 const uint32_t v = cur[e];
                 if (v >= s) {
                     atomicOr(status, kErrNotPermutation);
                     continue;
                 }
                 inv[path * cap + v] = (uint16_t)i;
-                if ((i & 1u) == 0) {
-                    const uint32_t id = path * pcap + (i >> 1);
-                    uf[id] = id << 1;
-                }
             }
             __syncthreads();
             // B: one union per output pair
@@ -196,8 +195,10 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
                     const uint32_t s = size_at(lv, level, first + path);
                     if (k < s / 2 && internal_node(path, s)) {
                         const uint32_t u = inv[path * cap + 2 * k];
-                        const uint32_t q = path * pcap + (u >> 1);
-                        y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                        if (u < s) { // an unwritten slot (repeated value) holds anything
+                            const uint32_t q = path * pcap + (u >> 1);
+                            y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                        }
                     }
                 }
                 const unsigned word = __ballot_sync(0xffffffffu, y);
@@ -297,6 +298,57 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
             break;
         }
     }
+}
+
+// One permutation: one CTA per node of the tile level.
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __restrict__ plan,
+    const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
+    uint32_t pairs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    tile_body<T>(plan, src, blob, status, slots, pairs, blockIdx.x, smem);
+}
+
+// Tiles of many permutations in one launch (the batched and serving forms):
+// job k owns blocks [first_block, first_block + tiles); the launch's dynamic
+// shared memory covers the largest job.
+// A job whose permutation is a single tile (tile level 0) also clears its
+// blob, writes the header and resets its status word first: its CTA is the
+// only writer of that blob.
+struct TileJob {
+    const Plan* plan;
+    const void* src;
+    uint32_t* blob;
+    uint32_t* status;
+    uint32_t slots;
+    uint32_t pairs;
+    uint32_t first_block;
+    uint32_t tiles;
+    uint32_t blob_words;   // words to clear (single-tile jobs)
+    uint32_t header_bytes;
+    uint8_t header[84];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kTileThreads, 2) tile_encode_batch(
+    const TileJob* __restrict__ jobs, uint32_t njobs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint32_t lo = 0, hi = njobs;
+    while (hi - lo > 1) { // last job whose first block is <= blockIdx.x
+        const uint32_t mid = (lo + hi) / 2;
+        if (jobs[mid].first_block <= blockIdx.x) lo = mid; else hi = mid;
+    }
+    const TileJob& job = jobs[lo];
+    if (job.tiles == 1 && job.blob_words != 0) {
+        for (uint32_t i = threadIdx.x; i < job.blob_words; i += blockDim.x) job.blob[i] = 0;
+        __syncthreads();
+        uint8_t* b = reinterpret_cast<uint8_t*>(job.blob);
+        for (uint32_t i = threadIdx.x; i < job.header_bytes; i += blockDim.x) b[i] = job.header[i];
+        if (threadIdx.x == 0) *job.status = 0;
+        __syncthreads();
+    }
+    tile_body<T>(job.plan, (const T*)job.src, job.blob, job.status, job.slots, job.pairs,
+        blockIdx.x - job.first_block, smem);
 }
 
 } // namespace bpb200

@@ -96,6 +96,62 @@ int bpb200_compress_device_noalloc(const void* d_entries, uint64_t count,
     uint32_t entry_bytes, const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len,
     void* stream, char* err, size_t err_len);
 
+/* ---------------------------------------------------------------- batched
+ * No reference counterpart (the reference compresses one permutation per
+ * call).  Compresses many device-resident permutations of uneven sizes in
+ * one call: every permutation of at most 8192 entries is encoded by a single
+ * batched launch (one CTA each); larger ones run their level kernels
+ * concurrently on pooled workspaces.  Each request's output bytes equal
+ * bpb200_compress_device's.  Per-request results land in `status`/`error`;
+ * the return value is the first failing status or BPB200_OK.
+ * `kernel_launches` (may be NULL) receives the number of kernel launches. */
+typedef struct bpb200_request {
+    const void* d_entries;  /* device input: count values of entry_bytes */
+    uint64_t count;
+    uint32_t entry_bytes;   /* 4 or 8 */
+    uint32_t reserved;
+    bpb200_format format;
+    uint8_t* d_blob;        /* device output, 4-byte aligned, rounded-up size */
+    uint64_t blob_len;      /* bpb200_encoded_size */
+    int status;             /* out: BPB200_* */
+    char error[124];        /* out: message when status != 0 */
+} bpb200_request;
+
+int bpb200_compress_batch(bpb200_request* requests, uint32_t count, void* stream,
+    uint32_t* kernel_launches);
+
+/* ---------------------------------------------------------------- serving
+ * No reference counterpart.  A request loop on its own threads: requests
+ * (host input, host blob) are admitted in arrival order while their device
+ * footprint fits `hbm_budget_bytes`; single-tile requests admitted together
+ * are encoded by one batched launch (up to `max_batch` per launch), larger
+ * ones by up to `workers` concurrent worker threads; admission resumes as
+ * requests complete.  Input and blob memory must stay valid until
+ * bpb200_server_wait returns for the ticket.  Latency runs from submit to
+ * the blob being written. */
+typedef struct bpb200_server bpb200_server;
+
+typedef struct bpb200_server_stats {
+    uint64_t submitted;
+    uint64_t completed;
+    uint64_t failed;
+    uint64_t entries;          /* entries of completed requests */
+    uint64_t kernel_launches;
+    double p50_seconds;        /* latency percentiles of completed requests */
+    double p99_seconds;
+    double mean_seconds;
+} bpb200_server_stats;
+
+bpb200_server* bpb200_server_create(uint64_t hbm_budget_bytes, uint32_t max_batch,
+    uint32_t workers, char* err, size_t err_len);
+int bpb200_server_submit(bpb200_server* server, const void* entries, uint64_t count,
+    uint32_t entry_bytes, const bpb200_format* format, uint8_t* blob, uint64_t blob_len,
+    uint64_t* ticket);
+int bpb200_server_wait(bpb200_server* server, uint64_t ticket, double* latency_seconds,
+    char* err, size_t err_len);
+int bpb200_server_get_stats(bpb200_server* server, bpb200_server_stats* stats);
+void bpb200_server_destroy(bpb200_server* server);
+
 /* Seeded synthetic permutations used by the benchmark and the tests
  * (workload generator, not part of the reference).  kind: 0 Fisher-Yates
  * uniform, 1 Sattolo single cycle, 2 identity, 3 reverse, 4 bit reversal

@@ -1,0 +1,106 @@
+# SPDX-License-Identifier: Apache-2.0
+"""Batched and serving forms: every blob must be byte-identical to the plain
+per-request call on the same input, whether the request ran alone or mixed
+with others (sizes, widths and formats drawn like the mixed-stream
+configuration, scaled down)."""
+import concurrent.futures as cf
+import hashlib
+
+import numpy as np
+import pytest
+
+from helpers import b200_format, oracle_format
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixed(gpu, count, max_log2, seed):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(round(2 ** rng.uniform(4, max_log2)))
+        kind = int(rng.integers(0, 2))
+        dtype = np.uint32 if rng.integers(0, 2) == 0 else np.uint64
+        kw = dict(middle_group_log2=int(rng.choice([4, 5])),
+                  middle_placement=int(rng.integers(0, 3)))
+        perm = gpu.fill_permutation(gpu.PermutationKind(kind), seed * 100003 + i, n, dtype)
+        out.append((perm, kw))
+    return out
+
+
+def test_batch_device_matches_plain(gpu):
+    torch = pytest.importorskip("torch")
+    reqs = _mixed(gpu, 60, 17, 1)
+    items, keep, expected = [], [], []
+    for perm, kw in reqs:
+        fmt = b200_format(gpu, kw)
+        n = perm.size
+        size = gpu.encoded_size(n, fmt)
+        width = perm.dtype.itemsize
+        d_in = torch.from_numpy(perm.view(np.int64 if width == 8 else np.int32)).cuda()
+        d_blob = torch.full(((size + 3) // 4 * 4,), 0x5A, dtype=torch.uint8, device="cuda")
+        keep.append((d_in, d_blob, size))
+        items.append((d_in.data_ptr(), n, width, fmt, d_blob.data_ptr(), size))
+        expected.append(gpu.compress(perm, gpu.CompressOptions(format=fmt)))
+    statuses, launches = gpu.compress_batch_device(items)
+    assert all(s == 0 for s in statuses)
+    assert launches > 0
+    torch.cuda.synchronize()
+    for (d_in, d_blob, size), want in zip(keep, expected):
+        assert d_blob[:size].cpu().numpy().tobytes() == want
+
+
+def test_batch_small_only_single_launch(gpu, oracle):
+    torch = pytest.importorskip("torch")
+    items, keep, perms = [], [], []
+    for i in range(200):
+        n = 1 + (i * 37) % 8192
+        perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 900 + i, n)
+        fmt = gpu.FormatOptions()
+        size = gpu.encoded_size(n, fmt)
+        d_in = torch.from_numpy(perm.view(np.int32)).cuda()
+        d_blob = torch.empty(((size + 3) // 4 * 4,), dtype=torch.uint8, device="cuda")
+        keep.append((d_blob, size))
+        perms.append(perm)
+        items.append((d_in.data_ptr(), n, 4, fmt, d_blob.data_ptr(), size))
+        keep.append(d_in)
+    statuses, launches = gpu.compress_batch_device(items)
+    assert launches == 1  # every single-tile permutation in one launch
+    blobs = [k for k in keep if isinstance(k, tuple)]
+    for (d_blob, size), perm in zip(blobs, perms):
+        assert d_blob[:size].cpu().numpy().tobytes() == oracle.compress(perm)
+
+
+def test_server_mixed_equals_alone(gpu):
+    reqs = _mixed(gpu, 120, 19, 2)
+    alone = [hashlib.sha256(gpu.compress(p, gpu.CompressOptions(format=b200_format(gpu, kw))))
+             .hexdigest() for p, kw in reqs]
+    with gpu.Server(hbm_budget_bytes=2 * 10**9, max_batch=64, workers=3) as server:
+        # submit from several threads at once so requests overlap on the device
+        def submit(item):
+            perm, kw = item
+            return server.submit(perm, gpu.CompressOptions(format=b200_format(gpu, kw)))
+        with cf.ThreadPoolExecutor(4) as pool:
+            tickets = list(pool.map(submit, reqs))
+        results = [server.wait(t) for t in tickets]
+        stats = server.stats()
+    for (blob, latency), want in zip(results, alone):
+        assert hashlib.sha256(blob).hexdigest() == want
+        assert latency > 0
+    assert stats["completed"] == len(reqs)
+    assert stats["p99_seconds"] >= stats["p50_seconds"] > 0
+
+
+def test_server_rejects_bad_request_without_harming_others(gpu, oracle):
+    good = gpu.fill_permutation(gpu.PermutationKind.uniform, 3, 5000)
+    bad = good.copy()
+    bad[10] = bad[11]
+    big = gpu.fill_permutation(gpu.PermutationKind.single_cycle, 4, 70000)
+    with gpu.Server(hbm_budget_bytes=10**9) as server:
+        t1 = server.submit(good)
+        t2 = server.submit(bad)
+        t3 = server.submit(big)
+        assert server.wait(t1)[0] == oracle.compress(good)
+        with pytest.raises(ValueError):
+            server.wait(t2)
+        assert server.wait(t3)[0] == oracle.compress(big)

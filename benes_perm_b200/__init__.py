@@ -7,8 +7,9 @@ Mirrors the reference's public compression API (include/benes/benes.hpp:
 through the C ABI in ``include/benes_b200.h`` into ``libbenes_b200.so``; there
 is no CPU fallback.  Errors raise the Python counterparts of the reference's
 exception types: ``ValueError`` for std::invalid_argument, ``OverflowError``
-for std::overflow_error, ``MemoryError``-free ``LengthError`` for
-std::length_error and ``RuntimeError`` for std::runtime_error.
+for std::overflow_error, ``LengthError`` (a ``ValueError`` subclass, as
+std::length_error derives from std::logic_error) for std::length_error and
+``RuntimeError`` for std::runtime_error.
 """
 from __future__ import annotations
 
@@ -124,6 +125,9 @@ def library() -> ctypes.CDLL:
                                                fp, ctypes.c_void_p, ctypes.c_uint64,
                                                ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                ctypes.c_char_p, ctypes.c_size_t]
+        lib.bpb200_compress_file.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32,
+                                             fp, ctypes.POINTER(ctypes.c_double),
+                                             ctypes.c_char_p, ctypes.c_size_t]
         lib.bpb200_fill_permutation.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
                                                 ctypes.c_uint32, ctypes.c_void_p]
         lib.bpb200_probe_switch_bit.argtypes = [ctypes.c_uint64, fp, ctypes.c_int, ctypes.c_uint32,
@@ -224,6 +228,24 @@ def compress(permutation, options: Optional[CompressOptions] = None,
     raise_for(rc, err.value.decode())
     _last_device_seconds = secs.value
     return blob if out is not None else blob.tobytes()
+
+
+def compress_file(input, output, input_width: InputValueWidth = InputValueWidth.bits64,
+                  options: Optional[CompressOptions] = None) -> None:
+    """benes::compress_file(input, output, input_width, {.backend = b200, ...})
+    (src/benes.cpp:498-553): encodes a raw little-endian permutation file and
+    writes the blob to ``output``.  The file is streamed to the device through
+    pinned chunks; the output is created only after the encode succeeded."""
+    global _last_device_seconds
+    options = options or CompressOptions()
+    cf = to_c_format(options.format)
+    err = ctypes.create_string_buffer(512)
+    secs = ctypes.c_double(0)
+    rc = library().bpb200_compress_file(os.fsencode(input), os.fsencode(output),
+                                        int(input_width), ctypes.byref(cf), ctypes.byref(secs),
+                                        err, 512)
+    raise_for(rc, err.value.decode())
+    _last_device_seconds = secs.value
 
 
 KERNEL_KINDS = ("prologue", "inverse", "descriptors", "union", "orient", "resolve",

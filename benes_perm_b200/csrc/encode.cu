@@ -381,7 +381,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
                 w.state[0], ctl);
             level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner, ctl);
         });
-        // rulers of one orbit lie in one node: at most cap/32 + 2 of them
+        // rulers of one orbit lie in one node: at most (cap >> kRulerLog2) + 2
         uint32_t rounds = 1;
         while ((1ull << rounds) < (lv.cap >> kRulerLog2) + 2) {
             ++rounds;
@@ -395,7 +395,8 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         });
     }
     rec.launch(kKindUnion, [&] {
-        level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
+        level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard,
+            ctl + kCtlClaimUnion, w.d_status);
     });
     rec.launch(kKindOrient, [&] {
         level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
@@ -624,6 +625,8 @@ int guarded(char* err, size_t err_len, Fn&& fn) {
     }
 }
 
+void destroy_rings(); // pinned file-staging rings (file.inc)
+
 } // namespace
 } // namespace bpb200
 
@@ -777,6 +780,7 @@ void bpb200_shutdown(void) {
     g_pool.erase(std::remove_if(g_pool.begin(), g_pool.end(),
                      [](const std::unique_ptr<Workspace>& w) { return w->device < 0; }),
         g_pool.end());
+    destroy_rings();
 }
 
 int bpb200_probe_switch_bit(uint64_t count, const bpb200_format* format, int side,
@@ -859,7 +863,7 @@ constexpr size_t kOffOwner = kOffAddr1 + up256(kNodes * sizeof(NodeAddress));
 constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
 constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffControl = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
-constexpr size_t kBytes = kOffControl + 256; // about 5.5 MB
+constexpr size_t kBytes = kOffControl + 256; // under 6 MB
 
 } // namespace noalloc
 } // namespace bpb200
@@ -985,3 +989,6 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
 
 // Batched and serving forms (share this file's pool, planning and launches).
 #include "serve.inc"
+
+// File form: streamed file -> device -> file (compress_file).
+#include "file.inc"

@@ -128,12 +128,19 @@ __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ pl
 //                 land in (block-local counts in shared memory, one global
 //                 reservation per block and window);
 //   level_place   replays each window's records; the writes of one window
-//                 stay inside an L2-resident 8 MB range.
+//                 stay inside an L2-resident 32 MB range.
+// Windows of 2^23 slots measured fastest on B200 at 2^30 uniform entries
+// (2^21: 256 ms of inverse per compress, 2^22: 240, 2^23: 226): larger
+// windows give each block longer runs of records per window.
 // A window receives at most as many records as it has slots when the input
 // is a permutation; an overfull window means a repeated value.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kPlaceLog2 = 21;
+#ifndef BPB200_PLACE_LOG2
+#define BPB200_PLACE_LOG2 23
+#endif
+constexpr uint32_t kPlaceLog2 = BPB200_PLACE_LOG2; // slots per destination window (log2)
 constexpr uint32_t kMaxWindows = 2048;
+static_assert((1ull << 31) >> kPlaceLog2 <= kMaxWindows, "windows must cover 2^31 slots");
 constexpr int kBucketItems = 16;
 
 template <typename T>
@@ -238,9 +245,13 @@ __global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan
     }
 }
 
+// Blocks claim chunks of output pairs in address order (claim_chunk), so the
+// union-find words being linked at any time belong to the few nodes those
+// chunks cover: once a node's words fit in L2 the random finds hit there.
+// `hard` was written by earlier launches: all threads see the same value.
 __global__ void __launch_bounds__(256) level_union(const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard,
-    uint32_t* status) {
+    uint32_t* claims, uint32_t* status) {
     if (hard != nullptr && *hard == 0) {
         return; // the orbit walks coloured this level
     }
@@ -248,9 +259,12 @@ __global__ void __launch_bounds__(256) level_union(const Plan* __restrict__ plan
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t total = (uint64_t)pcap << level;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kUnionItems;
-    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kUnionItems;
-         p0 < total; p0 += stride) {
+    uint64_t first;
+    while (claim_chunk(claims, (uint64_t)blockDim.x * kUnionItems, total, &first)) {
+        const uint64_t p0 = first + (uint64_t)threadIdx.x * kUnionItems;
+        if (p0 >= total) {
+            continue;
+        }
         uint32_t j = (uint32_t)(p0 / pcap);
         uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
         uint32_t s = size_at(lv, level, j);

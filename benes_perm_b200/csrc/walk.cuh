@@ -39,10 +39,24 @@
 
 namespace bpb200 {
 
-constexpr uint32_t kRulerLog2 = 5;           // one ruler per 32 slots
+// Tuning knobs, overridable at build time.  Measured on B200 over uniform
+// 2^28-entry inputs: one ruler per 16 slots and walks up to 2^23-entry nodes
+// gave the lowest total (rulers per 8 or 32 slots, and limits of 2^22 or
+// 2^24, were 1-4% slower).
+#ifndef BPB200_RULER_LOG2
+#define BPB200_RULER_LOG2 4
+#endif
+#ifndef BPB200_WALK_MAX_LOG2
+#define BPB200_WALK_MAX_LOG2 23
+#endif
+
+constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
 constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
 constexpr uint32_t kWalkChunk = 16;          // rulers claimed per warp at a time
-constexpr uint64_t kWalkMaxNode = 1ull << 22; // larger nodes are coloured by union-find
+constexpr uint32_t kJumpItems = 8;           // rulers per thread in a claimed jump chunk
+constexpr uint64_t kWalkMaxNode = 1ull << BPB200_WALK_MAX_LOG2; // larger: union-find
+static_assert(BPB200_RULER_LOG2 >= 2 && BPB200_RULER_LOG2 <= 8, "ruler density out of range");
+static_assert(BPB200_WALK_MAX_LOG2 >= 13 && BPB200_WALK_MAX_LOG2 <= 28, "walk limit out of range");
 constexpr uint32_t kUnset = 0xffffffffu;     // owner of a vertex no walk reached
 constexpr uint32_t kColourTag = 0x80000000u; // owner value carrying a colour directly
 constexpr uint32_t kNoRuler = 0xffffffffu;   // bucket whose hashed slot is padding
@@ -56,7 +70,10 @@ enum : int {
     kCtlClaim = 4,       // ruler chunks handed out by level_walk
     kCtlClaimPlace = 5,  // chunks handed out by level_place
     kCtlClaimInverse = 6, // chunks handed out by level_inverse
-    kCtlWords = 8
+    kCtlClaimJump = 7,   // ruler chunks handed out by ruler_jump (reset every round)
+    kCtlClaimUnion = 8,  // chunks handed out by level_union
+    kCtlClaimFinal = 9,  // chunks handed out by level_finalize
+    kCtlWords = 16       // control_reset clears them with one warp
 };
 
 __device__ __forceinline__ uint32_t ruler_position(uint32_t bucket) {
@@ -259,7 +276,11 @@ __global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__
     }
 }
 
-// One pointer-jumping round over ruler states (src -> dst).
+// One pointer-jumping round over ruler states (src -> dst).  Blocks claim
+// chunks of rulers in address order, so the rulers being jumped at any time
+// (and, early on, the near successors they read) stay close together.
+// The done/hard words were written by earlier launches, so every thread of
+// a block sees the same value and the block leaves together.
 __global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
     uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
@@ -267,17 +288,24 @@ __global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
         return;
     }
     bool changed = false;
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rulers;
-         r += gridDim.x * blockDim.x) {
-        const uint4 me = src[r];
-        if (me.x == kNoRuler) {
-            dst[r] = me;
-            continue;
+    const uint64_t chunk = (uint64_t)blockDim.x * kJumpItems;
+    uint64_t first = 0;
+    while (claim_chunk(control + kCtlClaimJump, chunk, rulers, &first)) {
+        for (uint32_t k = 0; k < kJumpItems; ++k) {
+            const uint64_t r = first + (uint64_t)k * blockDim.x + threadIdx.x;
+            if (r >= rulers) {
+                break;
+            }
+            const uint4 me = src[r];
+            if (me.x == kNoRuler) {
+                dst[r] = me;
+                continue;
+            }
+            const uint4 nx = src[me.x];
+            const uint4 out = make_uint4(nx.x, min(me.y, nx.y), min(me.z, nx.z), 0);
+            changed |= (out.y != me.y) || (out.z != me.z);
+            dst[r] = out;
         }
-        const uint4 nx = src[me.x];
-        const uint4 out = make_uint4(nx.x, min(me.y, nx.y), min(me.z, nx.z), 0);
-        changed |= (out.y != me.y) || (out.z != me.z);
-        dst[r] = out;
     }
     if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) {
         atomicOr(control + kCtlChanged, 1u);
@@ -288,6 +316,7 @@ __global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
 // After a round: a round that changed nothing means every ruler holds its
 // orbit's minima; later rounds then return at once.
 __global__ void ruler_check(uint32_t round, uint32_t* control) {
+    control[kCtlClaimJump] = 0; // the next round claims from the start again
     if (control[kCtlDone] != 0 || control[kCtlHard] != 0) {
         return;
     }
@@ -307,12 +336,15 @@ __global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
 }
 
 // Colours (from the walks, or from union-find when the level fell back),
-// children and the colour bitmap: thread per 4 pair-nodes.
+// children and the colour bitmap: thread per 4 pair-nodes.  Blocks claim
+// chunks in address order so the finds (or ruler-state reads) of a chunk
+// stay within the nodes it covers.  Every thread of a block runs every
+// claimed chunk (the colour bitmap is assembled with warp shuffles).
 template <typename T>
 __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
     const uint4* __restrict__ state0, const uint4* __restrict__ state1, uint32_t* uf,
-    uint32_t* __restrict__ xbits, uint32_t* __restrict__ dst, const uint32_t* control,
+    uint32_t* __restrict__ xbits, uint32_t* __restrict__ dst, uint32_t* control,
     uint32_t* status) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
@@ -322,9 +354,25 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
     const bool hard = control[kCtlHard] != 0;
     const uint4* state = control[kCtlFinal] ? state1 : state0;
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kResolveItems;
-    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kResolveItems;
-         p0 - lane * kResolveItems < total; p0 += stride) {
+    const uint64_t chunk = (uint64_t)blockDim.x * kResolveItems;
+    // Walk levels claim chunks in order (ruler states of the nodes in flight
+    // stay in L2).  Union-find levels stride over the whole level instead:
+    // claimed chunks would crowd every find in flight onto the root chains
+    // of one node's few large components, and those words then serialise.
+    uint64_t first = (uint64_t)blockIdx.x * chunk;
+    bool started = false;
+    auto next_chunk = [&]() -> bool {
+        if (!hard) {
+            return claim_chunk(control + kCtlClaimFinal, chunk, total, &first);
+        }
+        if (started) {
+            first += (uint64_t)gridDim.x * chunk;
+        }
+        started = true;
+        return first < total;
+    };
+    while (next_chunk()) {
+        const uint64_t p0 = first + (uint64_t)threadIdx.x * kResolveItems;
         uint32_t j = (uint32_t)(p0 / pcap);
         uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
         uint32_t s = size_at(lv, level, j);

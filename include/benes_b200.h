@@ -83,7 +83,7 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
  * allocation can imply.  Same arguments and result bytes as
  * bpb200_compress_device (device input and blob, work queued on `stream`),
  * but every byte of scratch comes from one fixed device array inside this
- * library (about 5.5 MB, present on every GPU that loads the library until
+ * library (under 6 MB, present on every GPU that loads the library until
  * the process exits), so it accepts at most 262144 (2^18) entries and
  * returns BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.
  * The first call on each device looks up the array's device address
@@ -95,6 +95,23 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
 int bpb200_compress_device_noalloc(const void* d_entries, uint64_t count,
     uint32_t entry_bytes, const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len,
     void* stream, char* err, size_t err_len);
+
+/* Replaces benes::compress_file (src/benes.cpp:498-553) for the b200
+ * backend: encodes the raw little-endian permutation file `input_path`
+ * (values of `input_width` = 4 or 8 bytes, the InputValueWidth values) and
+ * writes the blob to `output_path`, byte-identical to compress_file with the
+ * portable backend.  The file is streamed to the device through pinned
+ * chunks (reads overlap the upload; there is no host decode pass) and the
+ * blob streamed back the same way.  Errors, in the reference's order:
+ * RUNTIME "cannot open permutation input file"; INVALID_ARGUMENT
+ * "permutation input has an invalid element width or size" (width not 4/8,
+ * empty file, size not a multiple of the width); UNAVAILABLE without a
+ * usable GPU; RUNTIME "failed to read permutation input file"; then every
+ * error of bpb200_compress; RUNTIME "failed to write compressed permutation
+ * file".  The output file is created only after the encode succeeded. */
+int bpb200_compress_file(const char* input_path, const char* output_path,
+    uint32_t input_width, const bpb200_format* format, double* device_seconds,
+    char* err, size_t err_len);
 
 /* ---------------------------------------------------------------- batched
  * No reference counterpart (the reference compresses one permutation per

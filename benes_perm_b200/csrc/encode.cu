@@ -412,11 +412,20 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         const LevelSide& ls = lv.side[side];
         const uint32_t span_log2 = p.groups[side][ls.group].depth - ls.rel - 1;
         const uint64_t packets = (lv.cap / 2 + (1ull << span_log2) - 1) >> span_log2;
-        const int ge = grid_for(packets << (l + span_log2), kLevelThreads);
-        rec.launch(kKindEmit, [&] {
-            level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, side == 0 ? w.xbits : w.ybits,
-                w.addr[side], d_blob);
-        });
+        const uint32_t* bits = side == 0 ? w.xbits : w.ybits;
+        if (span_log2 >= 5) {
+            // runs of at least 32 switches: copy whole words
+            const int ge = grid_for(packets << (l + span_log2 - 5), kLevelThreads);
+            rec.launch(kKindEmit, [&] {
+                level_emit_words<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side],
+                    d_blob);
+            });
+        } else {
+            const int ge = grid_for(packets << (l + span_log2), kLevelThreads);
+            rec.launch(kKindEmit, [&] {
+                level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side], d_blob);
+            });
+        }
     }
     check(cudaGetLastError(), "level kernel launch");
 }

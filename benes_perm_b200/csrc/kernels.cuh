@@ -35,7 +35,17 @@ namespace bpb200 {
 constexpr uint32_t kNodeWave = 256;   // node descriptors held in shared memory at once
 constexpr uint32_t kTileThreads = 512;
 constexpr int kInverseItems = 8;      // slots per thread in level_inverse
-constexpr int kUnionItems = 4;        // output pairs per thread in level_union
+// level_union shape: 2 output pairs per thread with at most 64 registers (4
+// blocks of 256 per SM) measured fastest on B200 at 2^30 uniform entries
+// (union kernels 253 ms per compress; 4 pairs at 100 registers: 304 ms;
+// 8 pairs: 420 ms).  More resident warps hide more of the random latency.
+#ifndef BPB200_UNION_ITEMS
+#define BPB200_UNION_ITEMS 2
+#endif
+#ifndef BPB200_UNION_MIN_BLOCKS
+#define BPB200_UNION_MIN_BLOCKS 4
+#endif
+constexpr int kUnionItems = BPB200_UNION_ITEMS; // output pairs per thread in level_union
 constexpr int kResolveItems = 4;      // pair-nodes per thread in level_resolve
 
 struct TileShape {
@@ -249,7 +259,7 @@ __global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan
 // union-find words being linked at any time belong to the few nodes those
 // chunks cover: once a node's words fit in L2 the random finds hit there.
 // `hard` was written by earlier launches: all threads see the same value.
-__global__ void __launch_bounds__(256) level_union(const Plan* __restrict__ plan,
+__global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) level_union(const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard,
     uint32_t* claims, uint32_t* status) {
     if (hard != nullptr && *hard == 0) {
@@ -478,6 +488,57 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
             }
         }
         emit_bit(blob, dest, set, 0xffffffffu);
+    }
+}
+
+// Word-wise form of level_emit for levels whose packets carry at least 32
+// switches of each node (span_log2 >= 5).  The switches of one node inside
+// one packet are a contiguous run of the node's bits and land on a
+// contiguous run of blob bits (SwitchBitAddress::bit moves by one per pair
+// inside a packet), so the level is a set of bit-range copies: thread per
+// 32-switch chunk, one funnel shift to align the source and one or two
+// atomics for the destination words (neighbouring runs share edge words).
+// Chunks start at multiples of 32 pairs, so a chunk never crosses a packet.
+__global__ void __launch_bounds__(256) level_emit_words(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob) {
+    const LevelInfo& lv = plan->levels[level];
+    const LevelSide& ls = lv.side[side];
+    const GroupInfo& gi = plan->groups[side][ls.group];
+    const uint32_t span_log2 = gi.depth - ls.rel - 1;
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint64_t max_pairs = lv.cap / 2;
+    const uint64_t packets = (max_pairs + (1ull << span_log2) - 1) >> span_log2;
+    const uint32_t cshift = span_log2 - 5;  // log2(chunks per run)
+    const uint32_t shift = level + cshift;  // log2(nodes * chunks per run)
+    const uint64_t total = packets << shift;
+    const uint64_t section_bit = plan->section_offset[side] * 8;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const uint64_t packet = t >> shift;
+        const uint64_t rem = t & ((1ull << shift) - 1);
+        const uint32_t node = (uint32_t)(rem >> cshift);
+        const uint64_t pair0 = (packet << span_log2) + ((rem & ((1ull << cshift) - 1)) << 5);
+        const uint64_t half = size_at(lv, level, node) / 2;
+        if (pair0 >= half) {
+            continue;
+        }
+        const uint64_t q = (uint64_t)node * pcap + pair0;
+        // the bit arrays keep one spare word, so bits[w + 1] is always there
+        const uint64_t w = q >> 5;
+        uint32_t v = __funnelshift_r(bits[w], bits[w + 1], (uint32_t)(q & 31));
+        if (half - pair0 < 32) {
+            v &= (1u << (uint32_t)(half - pair0)) - 1u;
+        }
+        if (v == 0) {
+            continue;
+        }
+        const uint64_t dest = section_bit + switch_bit(addr[node], pair0);
+        const uint32_t off = (uint32_t)(dest & 31);
+        atomicOr(blob + (dest >> 5), v << off);
+        if (off != 0 && (v >> (32 - off)) != 0) {
+            atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
+        }
     }
 }
 

@@ -16,6 +16,18 @@ namespace bpb200 {
 
 __host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
 
+// Division by a per-level constant: floor(n / d) = umulhi(n, ceil(2^32 / d))
+// exactly whenever n * d < 2^32 (the rounding error n * (m - 2^32/d) / 2^32
+// stays below 1/d), which holds for tile indices: n and d are below 2^16.
+struct FastDiv {
+    uint32_t d, m;
+    __device__ explicit FastDiv(uint32_t div)
+        : d(div), m(div > 1 ? (uint32_t)((0x100000000ull + div - 1) / div) : 0u) {}
+    __device__ __forceinline__ uint32_t operator()(uint32_t n) const {
+        return d > 1 ? __umulhi(n, m) : n;
+    }
+};
+
 // Byte offsets of the smem arrays; identical on host (sizing) and device.
 __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pairs,
     uint32_t* off) {
@@ -80,6 +92,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
         const LevelInfo& lv = plan.levels[level];
         const uint32_t cap = (uint32_t)lv.cap;
         const uint32_t pcap = (uint32_t)lv.pcap;
+        const FastDiv by_cap(cap), by_pcap(pcap);
         const uint32_t nodes = 1u << t;
         const uint32_t first = J << t;
         uint16_t* cur = vals[t & 1];
@@ -104,7 +117,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             }
             // A: inverse and union-find init
             for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
-                const uint32_t path = e / cap;
+                const uint32_t path = by_cap(e);
                 const uint32_t i = e - path * cap;
                 const uint32_t s = size_at(lv, level, first + path);
                 if (i >= s || !internal_node(path, s)) {
@@ -124,7 +137,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             __syncthreads();
             // B: one union per output pair
             for (uint32_t p = tid; p < nodes * pcap; p += blockDim.x) {
-                const uint32_t path = p / pcap;
+                const uint32_t path = by_pcap(p);
                 const uint32_t k = p - path * pcap;
                 const uint32_t s = size_at(lv, level, first + path);
                 if (k >= s / 2 || !internal_node(path, s)) {
@@ -163,7 +176,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 const uint32_t p = base + lane;
                 uint32_t x = 0;
                 if (p < ptotal) {
-                    const uint32_t path = p / pcap;
+                    const uint32_t path = by_pcap(p);
                     const uint32_t k = p - path * pcap;
                     const uint32_t s = size_at(lv, level, first + path);
                     if (k < s - s / 2 && internal_node(path, s)) {
@@ -190,7 +203,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 const uint32_t p = base + lane;
                 bool y = false;
                 if (p < ptotal) {
-                    const uint32_t path = p / pcap;
+                    const uint32_t path = by_pcap(p);
                     const uint32_t k = p - path * pcap;
                     const uint32_t s = size_at(lv, level, first + path);
                     if (k < s / 2 && internal_node(path, s)) {
@@ -229,6 +242,41 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     const uint32_t total = packets << shift;
                     const uint32_t* bits = side == 0 ? xbits : ybits;
                     const uint64_t sec = plan.section_offset[side] * 8;
+                    if (span_log2 >= 5) {
+                        // runs of at least 32 switches: word-wise copies as in
+                        // level_emit_words (the bit arrays keep a spare word)
+                        const uint32_t cshift = span_log2 - 5;
+                        const uint32_t cs = wave_log2 + cshift;
+                        const uint32_t chunks = packets << cs;
+                        for (uint32_t c = tid; c < chunks; c += blockDim.x) {
+                            const uint32_t packet = c >> cs;
+                            const uint32_t rem = c & ((1u << cs) - 1);
+                            const uint32_t slot = rem >> cshift;
+                            const uint32_t pair0 =
+                                (packet << span_log2) + ((rem & ((1u << cshift) - 1)) << 5);
+                            const uint32_t path = w0 + slot;
+                            const uint32_t s = size_at(lv, level, first + path);
+                            if (pair0 >= s / 2 || !internal_node(path, s)) {
+                                continue;
+                            }
+                            const uint32_t q = path * pcap + pair0;
+                            uint32_t v = __funnelshift_r(bits[q >> 5], bits[(q >> 5) + 1], q & 31);
+                            if (s / 2 - pair0 < 32) {
+                                v &= (1u << (s / 2 - pair0)) - 1u;
+                            }
+                            if (v == 0) {
+                                continue;
+                            }
+                            const uint64_t dest =
+                                sec + switch_bit(desc[side * kNodeWave + slot], pair0);
+                            const uint32_t off = (uint32_t)(dest & 31);
+                            atomicOr(blob + (dest >> 5), v << off);
+                            if (off != 0 && (v >> (32 - off)) != 0) {
+                                atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
+                            }
+                        }
+                        continue;
+                    }
                     for (uint32_t base = warp * 32; base < total; base += nwarps * 32) {
                         const uint32_t tt = base + lane;
                         bool set = false;

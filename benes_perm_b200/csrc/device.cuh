@@ -102,9 +102,21 @@ __device__ __forceinline__ void uf_union(Word* uf, uint32_t a, uint32_t b, uint3
 // K finds advanced in lockstep: every round issues the loads of all
 // unfinished finds before using any of them, so one thread keeps up to 2K
 // independent loads in flight.  Bits of `pending` name the finds to run.
+// `cached`: plain (L1-cached) loads, for finds that run after every union
+// of the level is done.  Every find of a big component reads its root's
+// word; through L1 those reads stop queueing at the one L2 slice that holds
+// it.  No root changes any more, and a stale cached word is an older parent
+// pointer, i.e. still an ancestor with its true parity, so cached finds end
+// at the same roots with the same bits.  (During the unions a stale word
+// could name a former root; the union kernel keeps uncached loads.)
+template <typename Word>
+__device__ __forceinline__ Word uf_word(Word* uf, uint32_t i, bool cached) {
+    return cached ? uf[i] : uf_load(uf, i);
+}
+
 template <int K, typename Word>
 __device__ __forceinline__ void uf_find_many(Word* uf, const uint32_t (&x)[K], Found (&out)[K],
-    uint32_t pending, uint32_t* err) {
+    uint32_t pending, uint32_t* err, bool cached = false) {
     uint32_t cur[K], acc[K];
 #pragma unroll
     for (int i = 0; i < K; ++i) {
@@ -123,7 +135,7 @@ __device__ __forceinline__ void uf_find_many(Word* uf, const uint32_t (&x)[K], F
         uint32_t w[K], wp[K];
 #pragma unroll
         for (int i = 0; i < K; ++i) {
-            if (pending & (1u << i)) w[i] = (uint32_t)uf_load(uf, cur[i]);
+            if (pending & (1u << i)) w[i] = (uint32_t)uf_word(uf, cur[i], cached);
         }
 #pragma unroll
         for (int i = 0; i < K; ++i) {
@@ -133,7 +145,7 @@ __device__ __forceinline__ void uf_find_many(Word* uf, const uint32_t (&x)[K], F
                     out[i] = {cur[i], acc[i]};
                     pending &= ~(1u << i);
                 } else {
-                    wp[i] = (uint32_t)uf_load(uf, p);
+                    wp[i] = (uint32_t)uf_word(uf, p, cached);
                 }
             }
         }

@@ -396,10 +396,10 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
             Found f[kResolveItems];
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) x[q] = (uint32_t)(p0 + q);
-            uf_find_many<kResolveItems>(uf, x, f, live, status);
+            uf_find_many<kResolveItems>(uf, x, f, live, status, true);
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {
-                if (live & (1u << q)) c[q] = f[q].bit ^ (uf_load(uf, f[q].root) & 1u);
+                if (live & (1u << q)) c[q] = f[q].bit ^ (uf[f[q].root] & 1u);
             }
         } else {
             // ruler id (or direct colour) of vertex 2k, else of 2k+1

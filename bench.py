@@ -136,21 +136,45 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- roofline
 
-def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits):
-    """Compulsory HBM bytes per kernel kind for one compress (each input read
-    once and each output written once at its minimal width)."""
-    per = {k: 0.0 for k in ("inverse", "union", "resolve", "output_bits", "tile")}
+def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, walk_levels):
+    """Compulsory HBM bytes per kernel kind for one compress: every array a
+    kernel must touch, read once and written once at its minimal width.
+    Levels in `walk_levels` are coloured by orbit walks (walk + jump), the
+    other global levels by union-find (union)."""
+    kinds = ("inverse", "union", "walk", "jump", "resolve", "output_bits", "emit", "tile")
+    per = {k: 0.0 for k in kinds}
     for lvl in range(tile):
         w = entry_bytes if lvl == 0 else 4
-        per["inverse"] += (w + 4) * n             # read values, write inverse
-        per["union"] += 8 * n                      # read inverse, one word per pair read+written
-        per["resolve"] += (2 + w + 4) * n + n / 8  # union-find words, values, children, bits
+        per["inverse"] += (w + 4) * n              # read values, write inverse
+        if lvl in walk_levels:
+            per["walk"] += 12 * n                  # values, inverse, owner stamp per vertex
+            per["jump"] += 2 * n                   # ruler states (16 B per 16 slots) read+written
+            per["resolve"] += (4 + w + 4) * n + n / 8  # owners, values, children, bits
+        else:
+            per["union"] += 8 * n                  # inverse, one word per pair read+written
+            per["resolve"] += (2 + w + 4) * n + n / 8  # union-find words, values, children, bits
         per["output_bits"] += 2 * n + n / 8        # even inverse entries, bits
+        per["emit"] += n / 4                       # bits of both sides, read and placed
     w = entry_bytes if tile == 0 else 4
     per["tile"] = w * n + 2 * (depth - tile) * n / 16 + middle_bits / 8
     pipeline = (entry_bytes * n + 4 * n * max(depth - 1, 0) + 4 * n * depth
                 + 2 * switch_bits / 8 + 4 * n + middle_bits / 8)
     return per, pipeline
+
+
+def measured_traffic(kind, n, levels):
+    """DRAM bytes per step of `kind` from the committed ncu summary
+    (profiles/dram_traffic.json): bytes per entry per level, measured with ncu
+    on a smaller input and scaled by entries and by the number of levels that
+    run the kind here."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
+            table = json.load(f)
+        row = table["kinds"][kind]
+    except (OSError, KeyError, ValueError):
+        return None
+    return {"bytes_per_step": row["bytes_per_entry_per_level"] * n * levels,
+            "source": f"{table['source']}; {row['launch']}"}
 
 
 def load_peaks():
@@ -257,12 +281,25 @@ def b200_arm(args, world, rank, local):
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     stop = torch.cuda.Event(enable_timing=True)
+    # per-kernel device times come from the timed steps themselves: every
+    # launch is bracketed by CUDA events on its own stream (two event
+    # records per launch, well under 1 ms per step)
+    bp.set_profiling(True)
+    kernel_secs = {}
+    kernel_counts = {}
+    walk_levels = set()
     with ClockSampler(gpu_index) as clocks:
         start.record(stream)
         for _ in range(args.steps):
             step()
+            ks, kc, _ = bp.last_profile()
+            for k in ks:
+                kernel_secs[k] = kernel_secs.get(k, 0.0) + ks[k] / args.steps
+                kernel_counts[k] = kc[k]
+            walk_levels |= {lvl for kind, lvl, _ in bp.last_profile_launches() if kind == "walk"}
         stop.record(stream)
         torch.cuda.synchronize()
+    bp.set_profiling(False)
     if dist is not None:
         dist.barrier()
     secs = start.elapsed_time(stop) / 1e3
@@ -271,12 +308,6 @@ def b200_arm(args, world, rank, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         secs = float(t.item())
     value = n * args.steps * world / secs
-
-    # per-kernel device times (separate, untimed pass)
-    bp.set_profiling(True)
-    step()
-    kernel_secs, kernel_counts, _ = bp.last_profile()
-    bp.set_profiling(False)
 
     # end to end through the host entry point: pinned input in, pinned blob out
     host_blob = torch.empty(size, dtype=torch.uint8, pin_memory=True)
@@ -305,23 +336,28 @@ def b200_arm(args, world, rank, local):
             dist.destroy_process_group()
         return
 
-    # roofline of the dominant kernel kind
-    lay_switch = None
-    from benes_perm_b200 import library  # noqa: F401
+    # roofline of the dominant kernel kind: its algorithmic bytes over all of
+    # its launches in a step, divided by their summed event-timed durations
     switch_bits, middle_bits = _section_bits(n, fmt)
-    alg, pipeline_bytes = algorithmic_bytes(n, depth, tile, 8, switch_bits, middle_bits)
-    timed = {k: v for k, v in kernel_secs.items() if k in alg and v > 0}
+    alg, pipeline_bytes = algorithmic_bytes(n, depth, tile, 8, switch_bits, middle_bits,
+                                            walk_levels)
+    timed = {k: v for k, v in kernel_secs.items() if alg.get(k, 0) > 0 and v > 0}
     dominant = max(timed, key=timed.get)
     peak, peak_kind = load_peaks()
     achieved = alg[dominant] / timed[dominant] / 1e9
     total_kernel = sum(kernel_secs.values())
+    kind_levels = {"union": tile - len(walk_levels), "walk": len(walk_levels),
+                   "jump": len(walk_levels), "tile": 1}
+    traffic = measured_traffic(dominant, n, kind_levels.get(dominant, tile))
     roofline = {
         "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",
-        "traffic": None,
+        "traffic": traffic["bytes_per_step"] if traffic else None,
+        "traffic_source": traffic["source"] if traffic else None,
         "algorithmic_bytes_per_step": alg[dominant],
         "kernel_seconds_per_step": timed[dominant],
         "share_of_device_time": timed[dominant] / total_kernel,
+        "per_kind_gbs": {k: round(alg[k] / timed[k] / 1e9, 1) for k in timed},
     }
     pipeline = {
         "algorithmic_bytes": pipeline_bytes, "seconds": secs / args.steps,
@@ -341,7 +377,7 @@ def b200_arm(args, world, rank, local):
         "pipeline_roofline": pipeline,
         "kernel_seconds": {k: round(v, 6) for k, v in kernel_secs.items()},
         "kernel_launches": kernel_counts,
-        "levels": {"depth": depth, "tile_level": tile},
+        "levels": {"depth": depth, "tile_level": tile, "walk_levels": sorted(walk_levels)},
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(world)

@@ -49,6 +49,12 @@ namespace bpb200 {
 #ifndef BPB200_WALK_MAX_LOG2
 #define BPB200_WALK_MAX_LOG2 23
 #endif
+// Union-find levels whose nodes have at most 2^BPB200_FINAL_STRIDE_LOG2
+// slots finalize in grid-stride order, larger ones in claimed order (see
+// level_finalize); measured on B200 at 2^30 uniform entries.
+#ifndef BPB200_FINAL_STRIDE_LOG2
+#define BPB200_FINAL_STRIDE_LOG2 24
+#endif
 
 constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
 constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
@@ -356,13 +362,18 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t chunk = (uint64_t)blockDim.x * kResolveItems;
     // Walk levels claim chunks in order (ruler states of the nodes in flight
-    // stay in L2).  Union-find levels stride over the whole level instead:
-    // claimed chunks would crowd every find in flight onto the root chains
-    // of one node's few large components, and those words then serialise.
+    // stay in L2), and so do union-find levels with nodes far above L2 size
+    // (the finds of neighbouring chunks share the top of their trees).  On
+    // union-find levels with nodes near L2 size, claimed chunks would crowd
+    // every find in flight onto the root chains of one or two nodes' large
+    // components, which then serialise: those stride over the whole level
+    // (at 2^30 uniform entries, claimed order took 18.5 -> 12.5 ms on the
+    // 2^30-slot level but 14 -> 19 ms on 2^24-slot nodes).
     uint64_t first = (uint64_t)blockIdx.x * chunk;
     bool started = false;
+    const bool claimed = !hard || cap > (1ull << BPB200_FINAL_STRIDE_LOG2);
     auto next_chunk = [&]() -> bool {
-        if (!hard) {
+        if (claimed) {
             return claim_chunk(control + kCtlClaimFinal, chunk, total, &first);
         }
         if (started) {

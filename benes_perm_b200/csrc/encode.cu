@@ -76,7 +76,8 @@ struct Workspace {
     uint32_t* xbits = nullptr;
     uint32_t* ybits = nullptr;
     uint32_t* owner = nullptr;             // ruler id stamped on each walked vertex
-    uint4* state[2] = {nullptr, nullptr};  // ruler states, double-buffered for jumping
+    uint4* state[2] = {nullptr, nullptr};  // ruler states; [1] holds the super-ruler states
+    uint32_t* super_of = nullptr;          // super-ruler (or stamped colour) of each ruler
     uint32_t* control = nullptr;           // per-level control words (walk.cuh)
     uint2* records = nullptr;              // partitioned-inverse records (kernels.cuh)
     uint32_t* cursor = nullptr;            // fill level of each destination window
@@ -91,11 +92,13 @@ struct Workspace {
 
     void release_scratch() {
         for (void* p : {(void*)vals[0], (void*)vals[1], (void*)inv, (void*)uf, (void*)xbits,
-                 (void*)ybits, (void*)owner, (void*)state[0], (void*)state[1], (void*)control,
+                 (void*)ybits, (void*)owner, (void*)state[0], (void*)state[1], (void*)super_of,
+                 (void*)control,
                  (void*)records, (void*)cursor, (void*)addr[0], (void*)addr[1]}) {
             if (p) cudaFree(p);
         }
         vals[0] = vals[1] = inv = uf = xbits = ybits = owner = control = cursor = nullptr;
+        super_of = nullptr;
         records = nullptr;
         state[0] = state[1] = nullptr;
         addr[0] = addr[1] = nullptr;
@@ -176,6 +179,7 @@ void ensure_scratch(Workspace& w, const Plan& p) {
     const uint64_t buckets = (slots >> kRulerLog2) + 1;
     check(cudaMalloc(&w.state[0], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
     check(cudaMalloc(&w.state[1], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
+    check(cudaMalloc(&w.super_of, buckets * 4), "cudaMalloc(super rulers)");
     check(cudaMalloc(&w.control, kCtlWords * 4), "cudaMalloc(control)");
     if (p.levels[0].cap > kWalkMaxNode) {
         // only levels with nodes above L2 size use the partitioned inverse
@@ -381,15 +385,24 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
                 w.state[0], ctl);
             level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner, ctl);
         });
-        // rulers of one orbit lie in one node: at most (cap >> kRulerLog2) + 2
+        // super-rulers of one orbit lie in one node: at most
+        // (cap >> (kRulerLog2 + kSuperLog2)) + 2 of them
+        const uint32_t supers = (buckets + (1u << kSuperLog2) - 1) >> kSuperLog2;
         uint32_t rounds = 1;
-        while ((1ull << rounds) < (lv.cap >> kRulerLog2) + 2) {
+        while ((1ull << rounds) < (lv.cap >> (kRulerLog2 + kSuperLog2)) + 2) {
             ++rounds;
         }
+        uint4* sstate[2] = {w.state[1], w.state[1] + supers};
         rec.launch(kKindJump, [&] {
+            check(cudaMemsetAsync(w.super_of, 0xff, (uint64_t)buckets * 4, st),
+                "cudaMemsetAsync(super rulers)");
+            ruler_super_walk<<<grid_for(supers, kLevelThreads), kLevelThreads, 0, st>>>(
+                w.state[0], buckets, sstate[0], w.super_of, ctl);
+            ruler_super_short<<<gw, kLevelThreads, 0, st>>>(w.state[0], buckets, w.super_of, ctl);
+            const int gj = grid_for(supers, kLevelThreads);
             for (uint32_t r = 0; r <= rounds; ++r) {
-                ruler_jump<<<gw, kLevelThreads, 0, st>>>(w.state[r & 1], w.state[(r + 1) & 1],
-                    buckets, r, ctl);
+                ruler_jump<<<gj, kLevelThreads, 0, st>>>(sstate[r & 1], sstate[(r + 1) & 1],
+                    supers, r, ctl);
                 ruler_check<<<1, 1, 0, st>>>(r, ctl);
             }
         });
@@ -402,8 +415,9 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
     });
     rec.launch(kKindResolve, [&] {
-        level_finalize<TV><<<gr, kLevelThreads, 0, st>>>(dp, l, src, w.owner, w.state[0],
-            w.state[1], w.uf, w.xbits, dst, ctl, w.d_status);
+        const uint32_t supers = (buckets + (1u << kSuperLog2) - 1) >> kSuperLog2;
+        level_finalize<TV><<<gr, kLevelThreads, 0, st>>>(dp, l, src, w.owner, w.super_of,
+            w.state[1], w.state[1] + supers, w.uf, w.xbits, dst, ctl, w.d_status);
     });
     rec.launch(kKindOutputBits, [&] {
         level_ybits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.ybits);
@@ -871,7 +885,8 @@ constexpr size_t kOffAddr1 = kOffAddr0 + up256(kNodes * sizeof(NodeAddress));
 constexpr size_t kOffOwner = kOffAddr1 + up256(kNodes * sizeof(NodeAddress));
 constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
 constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
-constexpr size_t kOffControl = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
+constexpr size_t kOffSuper = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
+constexpr size_t kOffControl = kOffSuper + up256(((kSlots >> kRulerLog2) + 1) * 4);
 constexpr size_t kBytes = kOffControl + 256; // under 6 MB
 
 } // namespace noalloc
@@ -958,6 +973,7 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         w.owner = reinterpret_cast<uint32_t*>(base + noalloc::kOffOwner);
         w.state[0] = reinterpret_cast<uint4*>(base + noalloc::kOffState0);
         w.state[1] = reinterpret_cast<uint4*>(base + noalloc::kOffState1);
+        w.super_of = reinterpret_cast<uint32_t*>(base + noalloc::kOffSuper);
         w.control = reinterpret_cast<uint32_t*>(base + noalloc::kOffControl);
         cudaStream_t st = (cudaStream_t)stream;
         // The plan source is ordinary host memory: the copy is staged before

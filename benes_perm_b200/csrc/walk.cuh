@@ -79,6 +79,7 @@ enum : int {
     kCtlClaimJump = 7,   // ruler chunks handed out by ruler_jump (reset every round)
     kCtlClaimUnion = 8,  // chunks handed out by level_union
     kCtlClaimFinal = 9,  // chunks handed out by level_finalize
+    kCtlClaimSuper = 10, // super-ruler chunks handed out by ruler_super_walk
     kCtlWords = 16       // control_reset clears them with one warp
 };
 
@@ -333,6 +334,110 @@ __global__ void ruler_check(uint32_t round, uint32_t* control) {
     control[kCtlChanged] = 0;
 }
 
+// ---------------------------------------------------------------------------
+// Super-rulers.  Jumping over all rulers costs a full pass over their states
+// per round (about log2 of the rulers in an orbit rounds).  Instead every
+// ruler whose id is a multiple of 2^kSuperLog2 is a super-ruler: it follows
+// the ruler chain to the next super-ruler once (ruler_super_walk), folding
+// the segment minima and stamping super_of[r] on the rulers it passes; the
+// jumping then runs over the 2^kSuperLog2 times smaller super states.  Ruler
+// cycles without a super-ruler are closed by ruler_super_short, which stamps
+// their colour directly (kColourTag).  super_of[] starts at kUnset.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kSuperLog2 = 4;
+
+__global__ void __launch_bounds__(256) ruler_super_walk(const uint4* __restrict__ state,
+    uint32_t rulers, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
+    uint32_t* control) {
+    if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
+        return; // the level is coloured by union-find
+    }
+    const uint32_t supers = (rulers + (1u << kSuperLog2) - 1) >> kSuperLog2;
+    uint64_t first = 0;
+    while (claim_chunk(control + kCtlClaimSuper, blockDim.x, supers, &first)) {
+        const uint64_t i = first + threadIdx.x;
+        if (i >= supers) {
+            continue;
+        }
+        const uint32_t r = (uint32_t)i << kSuperLog2;
+        const uint4 me = state[r];
+        if (me.x == kNoRuler) {
+            sstate[i] = make_uint4(kNoRuler, 0, 0, 0);
+            continue;
+        }
+        super_of[r] = r;
+        uint32_t ma = me.y, mb = me.z, cur = me.x;
+        for (uint32_t hop = 0; (cur & ((1u << kSuperLog2) - 1)) != 0; ++hop) {
+            if (cur >= rulers || hop == kWalkCap) {
+                atomicOr(control + kCtlHard, 1u);
+                break;
+            }
+            const uint4 st = state[cur];
+            super_of[cur] = r;
+            ma = min(ma, st.y);
+            mb = min(mb, st.z);
+            cur = st.x;
+        }
+        sstate[i] = make_uint4(cur >> kSuperLog2, ma, mb, 0);
+    }
+}
+
+// Ruler cycles that contain no super-ruler: thread per ruler no super walk
+// reached; the ruler with the smallest id of its cycle folds the cycle's
+// minima and stamps the colour on every ruler of it.
+__global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict__ state,
+    uint32_t rulers, uint32_t* __restrict__ super_of, uint32_t* control) {
+    if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
+        return;
+    }
+    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rulers;
+         r += gridDim.x * blockDim.x) {
+        if (super_of[r] != kUnset) {
+            continue;
+        }
+        const uint4 me = state[r];
+        if (me.x == kNoRuler) {
+            continue;
+        }
+        uint32_t ma = me.y, mb = me.z, cur = me.x;
+        bool smallest = true, closed = false;
+        for (uint32_t hop = 0; hop < kWalkCap; ++hop) {
+            if (cur >= rulers) {
+                break;
+            }
+            if (cur == r) {
+                closed = true;
+                break;
+            }
+            if (cur < r) {
+                smallest = false; // that ruler's thread closes this cycle
+                closed = true;
+                break;
+            }
+            const uint4 st = state[cur];
+            ma = min(ma, st.y);
+            mb = min(mb, st.z);
+            cur = st.x;
+        }
+        if (!closed) {
+            atomicOr(control + kCtlHard, 1u);
+            continue;
+        }
+        if (!smallest) {
+            continue;
+        }
+        const uint32_t colour = kColourTag | (ma > mb ? 1u : 0u);
+        cur = r;
+        for (uint32_t hop = 0; hop < kWalkCap; ++hop) {
+            super_of[cur] = colour;
+            cur = state[cur].x;
+            if (cur == r || cur >= rulers) {
+                break;
+            }
+        }
+    }
+}
+
 // Clears the level's control words; `force_union_find` pre-sets the hard
 // flag so the level is coloured by union-find (a test hook for that path).
 __global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
@@ -349,7 +454,8 @@ __global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
 template <typename T>
 __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
-    const uint4* __restrict__ state0, const uint4* __restrict__ state1, uint32_t* uf,
+    const uint32_t* __restrict__ super_of, const uint4* __restrict__ state0,
+    const uint4* __restrict__ state1, uint32_t* uf,
     uint32_t* __restrict__ xbits, uint32_t* __restrict__ dst, uint32_t* control,
     uint32_t* status) {
     const LevelInfo& lv = plan->levels[level];
@@ -440,8 +546,18 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
                 } else if (id[q] & kColourTag) {
                     colour = id[q] & 1u;
                 } else {
-                    const uint4 st = state[id[q]];
-                    colour = st.y > st.z ? 1u : 0u;
+                    // ruler -> its super-ruler's orbit minima (or a colour
+                    // stamped on a super-free ruler cycle)
+                    const uint32_t so = super_of[id[q]];
+                    if (so == kUnset) {
+                        atomicOr(status, kErrInconsistent);
+                        colour = 0;
+                    } else if (so & kColourTag) {
+                        colour = so & 1u;
+                    } else {
+                        const uint4 st = state[so >> kSuperLog2];
+                        colour = st.y > st.z ? 1u : 0u;
+                    }
                 }
                 c[q] = colour ^ flip[q];
             }

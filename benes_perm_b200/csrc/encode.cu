@@ -263,7 +263,7 @@ std::atomic<int> g_force_union_find{0};
 int walk_blocks_per_sm() {
     static const int value = [] {
         const char* env = std::getenv("BPB200_WALK_BLOCKS_PER_SM");
-        const int v = env ? std::atoi(env) : 2;
+        const int v = env ? std::atoi(env) : 4;
         return v < 1 ? 1 : (v > 8 ? 8 : v);
     }();
     return value;
@@ -887,7 +887,7 @@ constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
 constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffSuper = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffControl = kOffSuper + up256(((kSlots >> kRulerLog2) + 1) * 4);
-constexpr size_t kBytes = kOffControl + 256; // under 6 MB
+constexpr size_t kBytes = kOffControl + 256; // under 7 MB
 
 } // namespace noalloc
 } // namespace bpb200

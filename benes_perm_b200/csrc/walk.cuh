@@ -40,11 +40,13 @@
 namespace bpb200 {
 
 // Tuning knobs, overridable at build time.  Measured on B200 over uniform
-// 2^28-entry inputs: one ruler per 16 slots and walks up to 2^23-entry nodes
-// gave the lowest total (rulers per 8 or 32 slots, and limits of 2^22 or
-// 2^24, were 1-4% slower).
+// 2^30-entry inputs with super-ruler jumping: one ruler per 8 slots, walks
+// up to 2^23-entry nodes and 4 walk blocks per SM gave the lowest total
+// (1078 ms; rulers per 16 slots: 1094 at 3 blocks per SM; per 32: 1175;
+// per 4: 1132; walk limit 2^24: 1112).  Denser rulers give shorter,
+// more numerous walk chains, which hide the L2 latency of each step better.
 #ifndef BPB200_RULER_LOG2
-#define BPB200_RULER_LOG2 4
+#define BPB200_RULER_LOG2 3
 #endif
 #ifndef BPB200_WALK_MAX_LOG2
 #define BPB200_WALK_MAX_LOG2 23

@@ -75,6 +75,26 @@ def workload_config(n, log2n, world):
     }
 
 
+def replica_seed(rank):
+    """Each replica compresses its own permutation (distinct seeds)."""
+    return SEED + rank
+
+
+def max_over_ranks(seconds, dist, device):
+    """The slowest rank's time: the job is done when every replica is."""
+    if dist is None:
+        return seconds
+    import torch
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(n, steps, world, seconds):
+    """Whole-job entries/s: every rank compresses `steps` permutations of n."""
+    return n * steps * world / seconds
+
+
 def dist_setup(gpus):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -162,18 +182,25 @@ def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, wal
     return per, pipeline
 
 
-def measured_traffic(kind, n, levels):
+def measured_traffic(kind, n, node_log2s):
     """DRAM bytes per step of `kind` from the committed ncu summary
-    (profiles/dram_traffic.json): bytes per entry per level, measured with ncu
-    on a smaller input and scaled by entries and by the number of levels that
-    run the kind here."""
+    (profiles/dram_traffic.json): bytes per entry of each level, measured
+    with ncu on a 2^26-entry input and keyed by the level's node size, summed
+    here over the levels that run the kind (`node_log2s`), times the entries.
+    Node sizes beyond the measured ones take the nearest measured size (a
+    node far above L2 size costs the same per entry at any size)."""
     try:
         with open(os.path.join(ROOT, "profiles", "dram_traffic.json")) as f:
             table = json.load(f)
         row = table["kinds"][kind]
     except (OSError, KeyError, ValueError):
         return None
-    return {"bytes_per_step": row["bytes_per_entry_per_level"] * n * levels,
+    known = {int(k): v for k, v in row["by_node_log2"].items()}
+
+    def per_entry(lg):
+        return known[min(known, key=lambda k: (abs(k - lg), k))]
+
+    return {"bytes_per_step": sum(per_entry(lg) for lg in node_log2s) * n,
             "source": f"{table['source']}; {row['launch']}"}
 
 
@@ -259,7 +286,7 @@ def b200_arm(args, world, rank, local):
 
     host = torch.empty(n, dtype=torch.int64, pin_memory=True)
     perm = host.numpy().view(np.uint64)
-    bp.fill_permutation(bp.PermutationKind.uniform, SEED + rank, n, np.uint64, out=perm)
+    bp.fill_permutation(bp.PermutationKind.uniform, replica_seed(rank), n, np.uint64, out=perm)
     d_in = host.to(f"cuda:{local}", non_blocking=False)
     d_blob = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
@@ -302,12 +329,8 @@ def b200_arm(args, world, rank, local):
     bp.set_profiling(False)
     if dist is not None:
         dist.barrier()
-    secs = start.elapsed_time(stop) / 1e3
-    if dist is not None:
-        t = torch.tensor([secs], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        secs = float(t.item())
-    value = n * args.steps * world / secs
+    secs = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, f"cuda:{local}")
+    value = replica_throughput(n, args.steps, world, secs)
 
     # end to end through the host entry point: pinned input in, pinned blob out
     host_blob = torch.empty(size, dtype=torch.uint8, pin_memory=True)
@@ -324,12 +347,8 @@ def b200_arm(args, world, rank, local):
         bp.compress(perm, opts, out=blob_np)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_secs = e0.elapsed_time(e1) / 1e3
-    if dist is not None:
-        t = torch.tensor([e2e_secs], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_secs = float(t.item())
-    e2e_value = n * args.e2e_steps * world / e2e_secs
+    e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, f"cuda:{local}")
+    e2e_value = replica_throughput(n, args.e2e_steps, world, e2e_secs)
 
     if rank != 0:
         if dist is not None:
@@ -346,9 +365,13 @@ def b200_arm(args, world, rank, local):
     peak, peak_kind = load_peaks()
     achieved = alg[dominant] / timed[dominant] / 1e9
     total_kernel = sum(kernel_secs.values())
-    kind_levels = {"union": tile - len(walk_levels), "walk": len(walk_levels),
-                   "jump": len(walk_levels), "tile": 1}
-    traffic = measured_traffic(dominant, n, kind_levels.get(dominant, tile))
+    node_log2 = {lvl: max(0, (-(-n >> lvl) - 1).bit_length()) for lvl in range(tile + 1)}
+    kind_levels = {"union": [node_log2[l] for l in range(tile) if l not in walk_levels],
+                   "walk": [node_log2[l] for l in sorted(walk_levels)],
+                   "jump": [node_log2[l] for l in sorted(walk_levels)],
+                   "tile": [node_log2[tile]]}
+    traffic = measured_traffic(dominant, n,
+                               kind_levels.get(dominant, [node_log2[l] for l in range(tile)]))
     roofline = {
         "bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "peak_source": f"{peak_kind} hbm_gbs",

@@ -302,9 +302,10 @@ struct Recorder {
         }
         return (*pool)[used++];
     }
+    // `kernels`: kernel launches f makes (counted in `launches`)
     template <typename F>
-    void launch(int kind, F&& f) {
-        ++launches;
+    void launch(int kind, F&& f, uint32_t kernels = 1) {
+        launches += kernels;
         if (!enabled) {
             f();
             return;
@@ -352,6 +353,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
     // nodes whose arrays do not fit in L2 are coloured by union-find
     const bool walks = lv.cap <= kWalkMaxNode && g_force_union_find.load() == 0;
     control_reset<<<1, 32, 0, st>>>(ctl, walks ? 0u : 1u);
+    rec.launches += 1;
     if (lv.cap > kWalkMaxNode && w.records != nullptr) {
         const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
         check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
@@ -361,7 +363,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
                 w.d_status);
             level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
                 w.records, w.cursor, w.inv, ctl + kCtlClaimPlace);
-        });
+        }, 2);
     } else {
         rec.launch(kKindInverse, [&] {
             level_inverse<TV><<<gs, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.uf, w.owner,
@@ -384,7 +386,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             level_walk<TV><<<gwalk, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner,
                 w.state[0], ctl);
             level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner, ctl);
-        });
+        }, 2);
         // super-rulers of one orbit lie in one node: at most
         // (cap >> (kRulerLog2 + kSuperLog2)) + 2 of them
         const uint32_t supers = (buckets + (1u << kSuperLog2) - 1) >> kSuperLog2;
@@ -405,7 +407,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
                     supers, r, ctl);
                 ruler_check<<<1, 1, 0, st>>>(r, ctl);
             }
-        });
+        }, 2 + 2 * (rounds + 1));
     }
     rec.launch(kKindUnion, [&] {
         level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard,

@@ -186,6 +186,22 @@ def encoded_size(count: int, fmt: Optional[FormatOptions] = None) -> int:
 
 _last_device_seconds = 0.0
 
+_bytes_new = ctypes.pythonapi.PyBytes_FromStringAndSize
+_bytes_new.restype = ctypes.py_object
+_bytes_new.argtypes = [ctypes.c_void_p, ctypes.c_ssize_t]
+_bytes_data = ctypes.pythonapi.PyBytes_AsString
+_bytes_data.restype = ctypes.c_void_p
+_bytes_data.argtypes = [ctypes.py_object]
+
+
+def _fresh_bytes(size: int):
+    """A new, not yet shared ``bytes`` object of ``size`` bytes and the address
+    of its contents, for the library to write the blob into: the C-API idiom
+    for building a bytes object in place, so the blob is not copied again
+    (fresh host pages are expensive to fault in, once is enough)."""
+    blob = _bytes_new(None, size)
+    return blob, _bytes_data(blob)
+
 
 def last_device_seconds() -> float:
     """detail::last_device_seconds() of the most recent compress call."""
@@ -218,16 +234,17 @@ def compress(permutation, options: Optional[CompressOptions] = None,
         if out.dtype != np.uint8 or out.size < size.value or not out.flags.c_contiguous:
             raise ValueError("out must be a contiguous uint8 array of the encoded size")
         blob = out[:size.value]
+        address = blob.ctypes.data
     else:
-        blob = np.empty(size.value, dtype=np.uint8)
+        blob, address = _fresh_bytes(size.value)
     secs = ctypes.c_double(0)
     rc = library().bpb200_compress(
         arr.ctypes.data, n, arr.dtype.itemsize, ctypes.byref(cf),
-        blob.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), size.value,
+        ctypes.cast(address, ctypes.POINTER(ctypes.c_uint8)), size.value,
         ctypes.byref(secs), err, 512)
     raise_for(rc, err.value.decode())
     _last_device_seconds = secs.value
-    return blob if out is not None else blob.tobytes()
+    return blob
 
 
 def compress_file(input, output, input_width: InputValueWidth = InputValueWidth.bits64,
@@ -391,11 +408,11 @@ class Server:
         if n == 0:
             raise ValueError("permutation size is out of range")
         size = encoded_size(n, options.format)
-        blob = np.empty(size, dtype=np.uint8)
+        blob, address = _fresh_bytes(size)
         cf = to_c_format(options.format)
         ticket = ctypes.c_uint64(0)
         rc = self._lib.bpb200_server_submit(self._handle, arr.ctypes.data, n, arr.dtype.itemsize,
-                                            ctypes.byref(cf), blob.ctypes.data, size,
+                                            ctypes.byref(cf), address, size,
                                             ctypes.byref(ticket))
         raise_for(rc, "submit failed")
         self._held[ticket.value] = (arr, blob, cf)
@@ -407,7 +424,7 @@ class Server:
         rc = self._lib.bpb200_server_wait(self._handle, ticket, ctypes.byref(latency), err, 256)
         _, blob, _ = self._held.pop(ticket, (None, None, None))
         raise_for(rc, err.value.decode())
-        return blob.tobytes(), latency.value
+        return blob, latency.value
 
     def stats(self) -> dict:
         s = _ServerStats()

@@ -156,19 +156,26 @@ struct Lease {
     ~Lease() { release(w); }
 };
 
+// Grows the level scratch to fit `p`.  Growth at least doubles the previous
+// capacities: freeing device memory synchronises the whole device, so a
+// workspace that serves requests of varying sizes (the batched and serving
+// forms) must reach its final size after a few calls, not one per call.
 void ensure_scratch(Workspace& w, const Plan& p) {
-    const uint64_t slots = p.tile_level > 0 ? p.max_slots : 0;
-    const uint64_t pairs = p.tile_level > 0 ? p.max_pairs : 0;
-    const uint64_t nodes = p.tile_level > 0 ? (1ull << (p.tile_level - 1)) : 0;
+    uint64_t slots = p.tile_level > 0 ? p.max_slots : 0;
+    uint64_t pairs = p.tile_level > 0 ? p.max_pairs : 0;
+    uint64_t nodes = p.tile_level > 0 ? (1ull << (p.tile_level - 1)) : 0;
     const bool need_records = p.levels[0].cap > kWalkMaxNode;
     if (slots <= w.slot_cap && pairs <= w.pair_cap && nodes <= w.node_cap &&
         (w.records != nullptr || !need_records)) {
         return;
     }
-    w.release_scratch();
     if (slots == 0) {
         return;
     }
+    slots = std::max(slots, 2 * w.slot_cap);
+    pairs = std::max(pairs, 2 * w.pair_cap);
+    nodes = std::max(nodes, 2 * w.node_cap);
+    w.release_scratch();
     check(cudaMalloc(&w.vals[0], slots * 4), "cudaMalloc(level array)");
     check(cudaMalloc(&w.vals[1], slots * 4), "cudaMalloc(level array)");
     check(cudaMalloc(&w.inv, slots * 4), "cudaMalloc(inverse)");
@@ -446,6 +453,27 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
     check(cudaGetLastError(), "level kernel launch");
 }
 
+// Raises a tile kernel's dynamic shared memory limit to the whole tile
+// budget, once per kernel and device.  Setting it per call to the call's own
+// size raced between concurrent callers: the limit is per function, and a
+// caller that lowered it between another caller's set and launch made that
+// launch fail ("too many resources requested").  The limit only bounds what
+// a launch may ask for; occupancy follows each launch's actual request.
+void allow_tile_smem(const void* kernel) {
+    static std::mutex m;
+    static std::vector<std::pair<const void*, int>> done;
+    int dev = 0;
+    check(cudaGetDevice(&dev), "cudaGetDevice");
+    std::lock_guard<std::mutex> lock(m);
+    for (const auto& d : done) {
+        if (d.first == kernel && d.second == dev) return;
+    }
+    check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+              (int)kTileSmemBudget),
+        "cudaFuncSetAttribute");
+    done.emplace_back(kernel, dev);
+}
+
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     const TileShape& shape, const T* d_in, uint32_t* d_blob) {
@@ -473,16 +501,13 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         throw CudaFail{cudaErrorInvalidValue, "too many tiles"};
     }
     if (t0 == 0) {
-        check(cudaFuncSetAttribute(tile_encode<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                  (int)shape.smem), "cudaFuncSetAttribute");
+        allow_tile_smem((const void*)tile_encode<T>);
         rec.launch(kKindTile, [&] {
             tile_encode<T><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, d_in, d_blob,
                 w.d_status, shape.slots, shape.pairs);
         });
     } else {
-        check(cudaFuncSetAttribute(tile_encode<uint32_t>,
-                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shape.smem),
-            "cudaFuncSetAttribute");
+        allow_tile_smem((const void*)tile_encode<uint32_t>);
         rec.launch(kKindTile, [&] {
             tile_encode<uint32_t><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, cur32,
                 d_blob, w.d_status, shape.slots, shape.pairs);
@@ -650,10 +675,33 @@ int guarded(char* err, size_t err_len, Fn&& fn) {
     }
 }
 
-void destroy_rings(); // pinned file-staging rings (file.inc)
+// Device staging of the host-path input and blob (grow-only).
+void ensure_staging(Workspace& w, uint64_t in_bytes, uint64_t blob_len) {
+    // grows at least twofold, like ensure_scratch
+    if (in_bytes > w.input_cap) {
+        const uint64_t cap = std::max(in_bytes, 2 * w.input_cap);
+        if (w.input) cudaFree(w.input);
+        w.input = nullptr;
+        w.input_cap = 0;
+        check(cudaMalloc(&w.input, cap), "cudaMalloc(input)");
+        w.input_cap = cap;
+    }
+    const uint64_t blob_bytes = ((blob_len + 3) / 4 + 1) * 4;
+    if (blob_bytes > w.blob_cap) {
+        const uint64_t cap = std::max(blob_bytes, 2 * w.blob_cap);
+        if (w.blob) cudaFree(w.blob);
+        w.blob = nullptr;
+        w.blob_cap = 0;
+        check(cudaMalloc(&w.blob, cap), "cudaMalloc(blob)");
+        w.blob_cap = cap;
+    }
+}
 
 } // namespace
 } // namespace bpb200
+
+// Pinned staging rings for host copies and files.
+#include "staging.inc"
 
 using namespace bpb200;
 
@@ -699,29 +747,43 @@ int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
             return rc;
         }
         const uint64_t in_bytes = count * entry_bytes;
-        if (in_bytes > w.input_cap) {
-            if (w.input) cudaFree(w.input);
-            w.input = nullptr;
-            w.input_cap = 0;
-            check(cudaMalloc(&w.input, in_bytes), "cudaMalloc(input)");
-            w.input_cap = in_bytes;
+        ensure_staging(w, in_bytes, blob_len);
+        // Pageable buffers of a few MB and more go through the pinned ring
+        // (parallel host copies overlapping the transfer); pinned ones and
+        // small ones are copied directly.
+        const bool stage_in = in_bytes >= kStageMin && !host_is_pinned(entries);
+        const bool stage_out = blob_len >= kStageMin && !host_is_pinned(blob);
+        std::unique_ptr<RingLease> ring;
+        if (stage_in || stage_out) {
+            ring = std::make_unique<RingLease>(device);
         }
-        const uint64_t blob_words = (blob_len + 3) / 4 + 1;
-        if (blob_words * 4 > w.blob_cap) {
-            if (w.blob) cudaFree(w.blob);
-            w.blob = nullptr;
-            w.blob_cap = 0;
-            check(cudaMalloc(&w.blob, blob_words * 4), "cudaMalloc(blob)");
-            w.blob_cap = blob_words * 4;
+        if (stage_in) {
+            const unsigned char* src = static_cast<const unsigned char*>(entries);
+            upload_staged(
+                [src](unsigned char* dst, uint64_t len, uint64_t off) {
+                    std::memcpy(dst, src + off, len);
+                    return true;
+                },
+                in_bytes, (unsigned char*)w.input, *ring->r, w.stream);
+        } else {
+            check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
+                "input upload");
         }
-        check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
-            "input upload");
         rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
         if (rc != kOk) {
             return rc;
         }
-        check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
-            "blob download");
+        if (stage_out) {
+            download_staged(
+                [blob](const unsigned char* src, uint64_t len, uint64_t off) {
+                    std::memcpy(blob + off, src, len);
+                    return true;
+                },
+                blob_len, (const unsigned char*)w.blob, *ring->r, w.stream);
+        } else {
+            check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
+                "blob download");
+        }
         check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
         return kOk;
     });

@@ -444,9 +444,24 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
                     d_blob);
             });
         } else {
-            const int ge = grid_for(packets << (l + span_log2), kLevelThreads);
+            // packets below the smallest node's tail packet: whole-word
+            // blocks; the rest (tail packets) bit by bit
+            const uint64_t half_min = lv.q / 2;
+            const uint64_t full = half_min >= 1 ? (half_min - 1) >> span_log2 : 0;
+            const uint32_t rel = ls.rel;
+            const uint32_t per_word_log2 = std::min<uint32_t>(5 - span_log2, rel);
+            if (full > 0) {
+                const uint64_t words = (full << (rel - per_word_log2)) << (l - rel);
+                rec.launch(kKindEmit, [&] {
+                    level_emit_blocks<<<grid_for(words, kLevelThreads), kLevelThreads, 0, st>>>(
+                        dp, l, side, bits, w.addr[side], d_blob, full);
+                });
+            }
+            const int ge = grid_for((packets - std::min(packets, full)) << (l + span_log2),
+                kLevelThreads);
             rec.launch(kKindEmit, [&] {
-                level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side], d_blob);
+                level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side], d_blob,
+                    full);
             });
         }
     }

@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(256) level_ybits(const Plan* __restrict__ plan
 // warp issues one or two atomics instead of one per bit.
 __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
     uint32_t level, int side, const uint32_t* __restrict__ bits,
-    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob) {
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t first_packet) {
     const LevelInfo& lv = plan->levels[level];
     const LevelSide& ls = lv.side[side];
     const GroupInfo& gi = plan->groups[side][ls.group];
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
     const uint64_t max_pairs = lv.cap / 2;
     const uint64_t packets = (max_pairs + (1ull << span_log2) - 1) >> span_log2;
     const uint32_t shift = level + span_log2; // log2(nodes * span)
-    const uint64_t total = packets << shift;
+    const uint64_t total = packets > first_packet ? (packets - first_packet) << shift : 0;
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -474,7 +474,7 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
         bool set = false;
         uint64_t dest = 0;
         if (t < total) {
-            const uint64_t packet = t >> shift;
+            const uint64_t packet = first_packet + (t >> shift);
             const uint64_t rem = t & ((1ull << shift) - 1);
             const uint32_t node = (uint32_t)(rem >> span_log2);
             const uint64_t pair = (packet << span_log2) + (rem & ((1ull << span_log2) - 1));
@@ -488,6 +488,58 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
             }
         }
         emit_bit(blob, dest, set, 0xffffffffu);
+    }
+}
+
+// Block form of level_emit for short runs (span_log2 < 5), on the packets
+// every node of the level fills (packet < full_packets: below the smallest
+// node's tail packet, so every node contributes `span` switches and every
+// path's run starts at path * span inside the packet, SectionAddress using
+// packet 0's prefix for all non-tail packets).  Inside such a packet the
+// level's switches of one cluster root are then one contiguous block,
+// path-major: thread per 32-bit word of a block, gathering the `span`-bit
+// fields of 32 / span consecutive nodes, one or two atomics per word.
+__global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
+    const LevelInfo& lv = plan->levels[level];
+    const LevelSide& ls = lv.side[side];
+    const GroupInfo& gi = plan->groups[side][ls.group];
+    const uint32_t rel = ls.rel;
+    const uint32_t span_log2 = gi.depth - rel - 1;
+    const uint32_t span_mask = (1u << (1u << span_log2)) - 1u; // span <= 16 bits
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    // nodes per word: 32 / span, or all 2^rel nodes of a root when fewer
+    const uint32_t per_word_log2 = min(5u - span_log2, rel);
+    const uint32_t words_log2 = rel - per_word_log2; // words per block (log2)
+    const uint64_t per_root = full_packets << words_log2;
+    const uint64_t total = (per_root << (level - rel));
+    const uint64_t section_bit = plan->section_offset[side] * 8;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+        const uint64_t root = t / per_root;
+        const uint64_t rem = t - root * per_root;
+        const uint64_t packet = rem >> words_log2;
+        const uint32_t word = (uint32_t)(rem & ((1ull << words_log2) - 1));
+        const uint32_t node0 = (uint32_t)(root << rel) + (word << per_word_log2);
+        uint32_t v = 0;
+        for (uint32_t i = 0; i < (1u << per_word_log2); ++i) {
+            const uint64_t q = (uint64_t)(node0 + i) * pcap + (packet << span_log2);
+            const uint64_t wq = q >> 5;
+            const uint32_t field =
+                __funnelshift_r(bits[wq], bits[wq + 1], (uint32_t)(q & 31)) & span_mask;
+            v |= field << (i << span_log2);
+        }
+        if (v == 0) {
+            continue;
+        }
+        const uint64_t dest = section_bit +
+            switch_bit(addr[(uint32_t)(root << rel)], packet << span_log2) + ((uint64_t)word << 5);
+        const uint32_t off = (uint32_t)(dest & 31);
+        atomicOr(blob + (dest >> 5), v << off);
+        if (off != 0 && (v >> (32 - off)) != 0) {
+            atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
+        }
     }
 }
 

@@ -282,12 +282,54 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                         }
                         continue;
                     }
-                    for (uint32_t base = warp * 32; base < total; base += nwarps * 32) {
+                    // short runs: the packets every node fills go out as
+                    // word blocks (see level_emit_blocks), the rest bit by bit
+                    uint32_t full = 0;
+                    if (all_internal && lv.q / 2 >= 1) {
+                        full = (uint32_t)(((lv.q / 2) - 1) >> span_log2);
+                    }
+                    if (full > packets) {
+                        full = packets;
+                    }
+                    if (full > 0) {
+                        const uint32_t rel = ls.rel;
+                        // nodes per word: within a word, a cluster root and the wave
+                        uint32_t g_log2 = 5 - span_log2;
+                        g_log2 = g_log2 < rel ? g_log2 : rel;
+                        g_log2 = g_log2 < wave_log2 ? g_log2 : wave_log2;
+                        const uint32_t span_mask = (1u << (1u << span_log2)) - 1u;
+                        const uint32_t groups_log2 = wave_log2 - g_log2;
+                        const uint32_t work = full << groups_log2;
+                        for (uint32_t c = tid; c < work; c += blockDim.x) {
+                            const uint32_t packet = c >> groups_log2;
+                            const uint32_t slot0 = (c & ((1u << groups_log2) - 1)) << g_log2;
+                            uint32_t v = 0;
+                            for (uint32_t i = 0; i < (1u << g_log2); ++i) {
+                                const uint32_t q = (w0 + slot0 + i) * pcap + (packet << span_log2);
+                                const uint32_t field =
+                                    __funnelshift_r(bits[q >> 5], bits[(q >> 5) + 1], q & 31) &
+                                    span_mask;
+                                v |= field << (i << span_log2);
+                            }
+                            if (v == 0) {
+                                continue;
+                            }
+                            const uint64_t dest = sec +
+                                switch_bit(desc[side * kNodeWave + slot0], packet << span_log2);
+                            const uint32_t off = (uint32_t)(dest & 31);
+                            atomicOr(blob + (dest >> 5), v << off);
+                            if (off != 0 && (v >> (32 - off)) != 0) {
+                                atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
+                            }
+                        }
+                    }
+                    const uint32_t rest = (packets - full) << shift;
+                    for (uint32_t base = warp * 32; base < rest; base += nwarps * 32) {
                         const uint32_t tt = base + lane;
                         bool set = false;
                         uint64_t dest = 0;
-                        if (tt < total) {
-                            const uint32_t packet = tt >> shift;
+                        if (tt < rest) {
+                            const uint32_t packet = full + (tt >> shift);
                             const uint32_t rem = tt & ((1u << shift) - 1);
                             const uint32_t slot = rem >> span_log2;
                             const uint32_t pair = (packet << span_log2) + (rem & ((1u << span_log2) - 1));

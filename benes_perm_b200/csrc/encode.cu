@@ -364,9 +364,9 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
     if (lv.cap > kWalkMaxNode && w.records != nullptr) {
         const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
         check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
-        const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kLevelThreads);
+        const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kBucketThreads);
         rec.launch(kKindInverse, [&] {
-            level_bucket<TV><<<gb, kLevelThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
+            level_bucket<TV><<<gb, kBucketThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
                 w.d_status);
             level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
                 w.records, w.cursor, w.inv, ctl + kCtlClaimPlace);

@@ -34,7 +34,14 @@ namespace bpb200 {
 
 constexpr uint32_t kNodeWave = 256;   // node descriptors held in shared memory at once
 constexpr uint32_t kTileThreads = 512;
-constexpr int kInverseItems = 8;      // slots per thread in level_inverse
+// 4 slots per thread measured fastest on B200 at 2^30 uniform entries
+// (inverse kernels 207 ms per compress; 8: 227 ms; 16: 243 ms): more
+// threads keep more of the scattered inverse stores in flight.
+#ifndef BPB200_INVERSE_ITEMS
+#define BPB200_INVERSE_ITEMS 4
+#endif
+static_assert(BPB200_INVERSE_ITEMS % 4 == 0, "level_inverse initialises owners 4 at a time");
+constexpr int kInverseItems = BPB200_INVERSE_ITEMS; // slots per thread in level_inverse
 // level_union shape: 2 output pairs per thread with at most 64 registers (4
 // blocks of 256 per SM) measured fastest on B200 at 2^30 uniform entries
 // (union kernels 253 ms per compress; 4 pairs at 100 registers: 304 ms;
@@ -46,7 +53,7 @@ constexpr int kInverseItems = 8;      // slots per thread in level_inverse
 #define BPB200_UNION_MIN_BLOCKS 4
 #endif
 constexpr int kUnionItems = BPB200_UNION_ITEMS; // output pairs per thread in level_union
-constexpr int kResolveItems = 4;      // pair-nodes per thread in level_resolve
+constexpr int kResolveItems = 4; // pair-nodes per thread in level_finalize (a nibble per lane)
 
 struct TileShape {
     uint32_t slots;   // padded entry slots needed at the deepest level
@@ -99,8 +106,10 @@ __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ pl
         // every slot starts unowned for the orbit walks
         if (e0 + kInverseItems <= total) {
             uint4* o = reinterpret_cast<uint4*>(owner + e0);
-            o[0] = make_uint4(~0u, ~0u, ~0u, ~0u);
-            o[1] = make_uint4(~0u, ~0u, ~0u, ~0u);
+#pragma unroll
+            for (int q = 0; q < kInverseItems / 4; ++q) {
+                o[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
+            }
         } else {
             for (uint64_t e = e0; e < total; ++e) owner[e] = ~0u;
         }
@@ -153,8 +162,13 @@ constexpr uint32_t kMaxWindows = 2048;
 static_assert((1ull << 31) >> kPlaceLog2 <= kMaxWindows, "windows must cover 2^31 slots");
 constexpr int kBucketItems = 16;
 
+#ifndef BPB200_BUCKET_THREADS
+#define BPB200_BUCKET_THREADS 256
+#endif
+constexpr int kBucketThreads = BPB200_BUCKET_THREADS; // block size of level_bucket
+
 template <typename T>
-__global__ void __launch_bounds__(256) level_bucket(const Plan* __restrict__ plan,
+__global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
     uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
     __shared__ uint32_t count[kMaxWindows];

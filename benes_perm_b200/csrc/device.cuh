@@ -343,14 +343,22 @@ __device__ __forceinline__ void emit_rank(uint32_t* blob, uint64_t abs, uint32_t
     }
     // bits of the rank that land in destination word `lane`
     const int lo_bit = (int)lane * 32 - (int)shift; // rank bit at dest bit 0 of this word
-    uint32_t v = 0;
-    for (int b = 0; b < 32; ++b) {
-        const int rb = lo_bit + b;
-        if (rb < 0 || rb >= (int)nbits) {
-            continue;
+    // rank < count! < 2^nbits, so no rank bit at or above nbits is set and
+    // the word is a plain 32-bit window of the 128-bit rank
+    uint32_t v;
+    if (lo_bit < 0) {
+        v = (uint32_t)(rank.lo << (uint32_t)(-lo_bit));
+    } else {
+        const uint32_t sh = (uint32_t)lo_bit; // < 128
+        unsigned long long x;
+        if (sh >= 64) {
+            x = rank.hi >> (sh - 64);
+        } else if (sh == 0) {
+            x = rank.lo;
+        } else {
+            x = (rank.lo >> sh) | (rank.hi << (64 - sh));
         }
-        const unsigned long long src = rb < 64 ? rank.lo : rank.hi;
-        v |= (uint32_t)((src >> (rb & 63)) & 1ull) << b;
+        v = (uint32_t)x;
     }
     if (v != 0) {
         atomicOr(blob + word0 + lane, v);

@@ -718,6 +718,70 @@ void ensure_staging(Workspace& w, uint64_t in_bytes, uint64_t blob_len) {
 // Pinned staging rings for host copies and files.
 #include "staging.inc"
 
+namespace bpb200 {
+namespace {
+
+// Host-memory compress (bpb200_compress): upload, encode, download.
+int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* blob, uint64_t blob_len, double* device_seconds,
+    char* err, size_t err_len) {
+    int device = 0;
+    if (!current_device_ok(&device)) {
+        set_error(err, err_len, "b200 backend is unavailable");
+        return kUnavailable;
+    }
+    Lease lease(device);
+    Workspace& w = *lease.w;
+    Call call;
+    int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+    if (rc != kOk) {
+        return rc;
+    }
+    const uint64_t in_bytes = count * entry_bytes;
+    ensure_staging(w, in_bytes, blob_len);
+    // Pageable buffers of a few MB and more go through the pinned ring
+    // (parallel host copies overlapping the transfer); pinned ones and
+    // small ones are copied directly.
+    const bool stage_in = in_bytes >= kStageMin && !host_is_pinned(entries);
+    const bool stage_out = blob_len >= kStageMin && !host_is_pinned(blob);
+    std::unique_ptr<RingLease> ring;
+    if (stage_in || stage_out) {
+        ring = std::make_unique<RingLease>(device);
+    }
+    if (stage_in) {
+        const unsigned char* src = static_cast<const unsigned char*>(entries);
+        upload_staged(
+            [src](unsigned char* dst, uint64_t len, uint64_t off) {
+                std::memcpy(dst, src + off, len);
+                return true;
+            },
+            in_bytes, (unsigned char*)w.input, *ring->r, w.stream);
+    } else {
+        check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
+            "input upload");
+    }
+    rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
+    if (rc != kOk) {
+        return rc;
+    }
+    if (stage_out) {
+        download_staged(
+            [blob](const unsigned char* src, uint64_t len, uint64_t off) {
+                std::memcpy(blob + off, src, len);
+                return true;
+            },
+            blob_len, (const unsigned char*)w.blob, *ring->r, w.stream);
+    } else {
+        check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
+            "blob download");
+    }
+    check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
+    return kOk;
+}
+
+} // namespace
+} // namespace bpb200
+
 using namespace bpb200;
 
 extern "C" {
@@ -749,58 +813,8 @@ int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
     const bpb200_format* format, uint8_t* blob, uint64_t blob_len, double* device_seconds,
     char* err, size_t err_len) {
     return guarded(err, err_len, [&]() -> int {
-        int device = 0;
-        if (!current_device_ok(&device)) {
-            set_error(err, err_len, "b200 backend is unavailable");
-            return kUnavailable;
-        }
-        Lease lease(device);
-        Workspace& w = *lease.w;
-        Call call;
-        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
-        if (rc != kOk) {
-            return rc;
-        }
-        const uint64_t in_bytes = count * entry_bytes;
-        ensure_staging(w, in_bytes, blob_len);
-        // Pageable buffers of a few MB and more go through the pinned ring
-        // (parallel host copies overlapping the transfer); pinned ones and
-        // small ones are copied directly.
-        const bool stage_in = in_bytes >= kStageMin && !host_is_pinned(entries);
-        const bool stage_out = blob_len >= kStageMin && !host_is_pinned(blob);
-        std::unique_ptr<RingLease> ring;
-        if (stage_in || stage_out) {
-            ring = std::make_unique<RingLease>(device);
-        }
-        if (stage_in) {
-            const unsigned char* src = static_cast<const unsigned char*>(entries);
-            upload_staged(
-                [src](unsigned char* dst, uint64_t len, uint64_t off) {
-                    std::memcpy(dst, src + off, len);
-                    return true;
-                },
-                in_bytes, (unsigned char*)w.input, *ring->r, w.stream);
-        } else {
-            check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
-                "input upload");
-        }
-        rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
-        if (rc != kOk) {
-            return rc;
-        }
-        if (stage_out) {
-            download_staged(
-                [blob](const unsigned char* src, uint64_t len, uint64_t off) {
-                    std::memcpy(blob + off, src, len);
-                    return true;
-                },
-                blob_len, (const unsigned char*)w.blob, *ring->r, w.stream);
-        } else {
-            check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
-                "blob download");
-        }
-        check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
-        return kOk;
+        return compress_host(entries, count, entry_bytes, format, blob, blob_len,
+            device_seconds, err, err_len);
     });
 }
 

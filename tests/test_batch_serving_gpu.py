@@ -104,3 +104,31 @@ def test_server_rejects_bad_request_without_harming_others(gpu, oracle):
         with pytest.raises(ValueError):
             server.wait(t2)
         assert server.wait(t3)[0] == oracle.compress(big)
+
+
+@pytest.mark.gpu
+def test_concurrent_host_calls_are_independent(gpu):
+    """The reference's compress is reentrant (one stream per call,
+    src/cuda/benes_cuda.cu:1192); calls from several host threads at once,
+    with inputs of different sizes and widths, give the bytes of the same
+    calls made one at a time."""
+    sizes = [(1 << 22) + 3, 70001, (1 << 20) + 17, 5000, (1 << 21), 3 * (1 << 19) + 1]
+    perms = [gpu.fill_permutation(gpu.PermutationKind.uniform, 40 + i, n,
+                                  np.uint64 if i % 2 else np.uint32)
+             for i, n in enumerate(sizes)]
+    alone = [gpu.compress(p) for p in perms]
+    with cf.ThreadPoolExecutor(len(perms)) as pool:
+        for _ in range(2):
+            assert list(pool.map(gpu.compress, perms)) == alone
+
+
+@pytest.mark.gpu
+def test_shrinking_then_growing_sizes(gpu, oracle):
+    """Workspaces grow geometrically and are reused: a large call, then small
+    ones, then a larger one must all stay byte-exact."""
+    for i, n in enumerate([1 << 21, 777, 40000, (1 << 22) + 5, 12345]):
+        perm = np.random.default_rng(200 + i).permutation(n)
+        if n <= 40000:
+            assert gpu.compress(perm.astype(np.uint64)) == oracle.compress(perm.astype(np.uint64))
+        else:
+            assert gpu.compress(perm.astype(np.uint32)) == gpu.compress(perm.astype(np.uint64))

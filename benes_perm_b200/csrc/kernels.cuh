@@ -13,16 +13,19 @@
 //                pair-nodes: colour(u) != colour(w) becomes
 //                x(u/2) ^ x(w/2) = 1 ^ (u&1) ^ (w&1), x(k) = colour(2k)
 //   orient       odd nodes: flip the tail's component so the tail is colour 0
-//   resolve      x(k) = parity to the component minimum (the canonical
-//                colouring: each component's smallest vertex gets colour 0);
+//   finalize     (walk.cuh) x(k) = parity to the component minimum (the
+//                canonical colouring: each component's smallest vertex gets
+//                colour 0), or the orbit-walk colour on walk levels;
 //                children left[k] = p[2k+x]/2, right[k] = p[2k+1-x]/2; the
 //                input switch of pair k is x(k)
 //   ybits        output switch of output pair k is colour(inv[2k])
-//   emit         switch bits into the clustered blob layout, in packet-major
-//                order so a warp's 32 lanes cover consecutive blob bits
+//   emit         switch bits into the clustered blob layout: word copies of
+//                long packet runs, word blocks of short ones, bits for the
+//                rest
 //
-// All loops keep several independent loads per thread in flight: the
-// kernels are bound by memory latency, not by instruction issue.
+// The kernels are bound by memory latency and random-access throughput, not
+// by instruction issue: their loops keep several independent loads per
+// thread in flight.
 #pragma once
 
 #include "device.cuh"
@@ -361,76 +364,6 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
          j += (uint64_t)gridDim.x * blockDim.x) {
         in_addr[j] = node_address(*plan, 0, level, j);
         out_addr[j] = node_address(*plan, 1, level, j);
-    }
-}
-
-// Colours of a warp-aligned run of 4*32 pair-nodes, children scatter.
-template <typename T>
-__global__ void __launch_bounds__(256) level_resolve(const Plan* __restrict__ plan,
-    uint32_t level, const T* __restrict__ src, uint32_t* uf, uint32_t* __restrict__ xbits,
-    uint32_t* __restrict__ dst, uint32_t* status) {
-    const LevelInfo& lv = plan->levels[level];
-    const uint32_t cap = (uint32_t)lv.cap;
-    const uint32_t pcap = (uint32_t)lv.pcap;
-    const uint32_t ccap = (uint32_t)plan->levels[level + 1].cap;
-    const uint64_t total = (uint64_t)pcap << level;
-    const uint32_t lane = threadIdx.x & 31;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x * kResolveItems;
-    for (uint64_t p0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * kResolveItems;
-         p0 - lane * kResolveItems < total; p0 += stride) {
-        uint32_t j = (uint32_t)(p0 / pcap);
-        uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
-        uint32_t s = size_at(lv, level, j);
-        uint32_t x[kResolveItems], jj[kResolveItems], kk[kResolveItems], ss[kResolveItems];
-        Found f[kResolveItems];
-        uint32_t pending = 0;
-#pragma unroll
-        for (int q = 0; q < kResolveItems; ++q) {
-            x[q] = (uint32_t)(p0 + q);
-            jj[q] = j;
-            kk[q] = k;
-            ss[q] = s;
-            if (p0 + q < total && k < s - s / 2) pending |= 1u << q;
-            if (++k == pcap) {
-                k = 0;
-                ++j;
-                s = size_at(lv, level, j);
-            }
-        }
-        const uint32_t live = pending;
-        uf_find_many<kResolveItems>(uf, x, f, pending, status);
-        uint32_t nibble = 0;
-        uint32_t flag[kResolveItems];
-#pragma unroll
-        for (int q = 0; q < kResolveItems; ++q) {
-            if (live & (1u << q)) flag[q] = uf_load(uf, f[q].root);
-        }
-#pragma unroll
-        for (int q = 0; q < kResolveItems; ++q) {
-            if (!(live & (1u << q))) continue;
-            const uint32_t c = f[q].bit ^ (flag[q] & 1u);
-            nibble |= c << q;
-            const uint64_t node = (uint64_t)jj[q] * cap;
-            const uint64_t left = (uint64_t)(2 * jj[q]) * ccap;
-            const uint64_t right = (uint64_t)(2 * jj[q] + 1) * ccap;
-            const uint32_t half = ss[q] / 2;
-            if (kk[q] < half) {
-                const uint32_t va = (uint32_t)src[node + 2 * kk[q] + c];
-                const uint32_t vb = (uint32_t)src[node + 2 * kk[q] + 1 - c];
-                dst[left + kk[q]] = va >> 1;
-                dst[right + kk[q]] = vb >> 1;
-            } else {
-                dst[left + kk[q]] = (uint32_t)(src[node + ss[q] - 1] >> 1);
-            }
-        }
-        // 8 lanes x 4 bits make one 32-bit word of colour bits
-        uint32_t v = nibble << ((lane & 7) * 4);
-        v |= __shfl_xor_sync(0xffffffffu, v, 1);
-        v |= __shfl_xor_sync(0xffffffffu, v, 2);
-        v |= __shfl_xor_sync(0xffffffffu, v, 4);
-        if ((lane & 7) == 0 && p0 < total) {
-            xbits[p0 >> 5] = v;
-        }
     }
 }
 

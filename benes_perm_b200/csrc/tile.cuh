@@ -244,7 +244,6 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     const uint32_t span_log2 = plan.groups[side][ls.group].depth - ls.rel - 1;
                     const uint32_t shift = wave_log2 + span_log2;
                     const uint32_t packets = (cap / 2 + (1u << span_log2) - 1) >> span_log2;
-                    const uint32_t total = packets << shift;
                     const uint32_t* bits = side == 0 ? xbits : ybits;
                     const uint64_t sec = plan.section_offset[side] * 8;
                     if (span_log2 >= 5) {

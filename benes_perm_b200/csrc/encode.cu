@@ -450,7 +450,15 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             const uint64_t full = half_min >= 1 ? (half_min - 1) >> span_log2 : 0;
             const uint32_t rel = ls.rel;
             const uint32_t per_word_log2 = std::min<uint32_t>(5 - span_log2, rel);
-            if (full > 0) {
+            if (full > 0 && rel >= 5) {
+                // roots of >= 32 nodes: warps of 32 nodes transpose their bits
+                const uint64_t windows = (full + (32 >> span_log2) - 1) >> (5 - span_log2);
+                const uint64_t threads = (windows << (l - 5)) * 32;
+                rec.launch(kKindEmit, [&] {
+                    level_emit_transpose<<<grid_for(threads, kLevelThreads), kLevelThreads, 0,
+                        st>>>(dp, l, side, bits, w.addr[side], d_blob, full);
+                });
+            } else if (full > 0) {
                 const uint64_t words = (full << (rel - per_word_log2)) << (l - rel);
                 rec.launch(kKindEmit, [&] {
                     level_emit_blocks<<<grid_for(words, kLevelThreads), kLevelThreads, 0, st>>>(

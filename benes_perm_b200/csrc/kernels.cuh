@@ -490,6 +490,67 @@ __global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict_
     }
 }
 
+// Transposed form of level_emit_blocks for cluster roots of at least 32
+// nodes (rel >= 5): a warp takes 32 consecutive nodes of one root and a
+// window of 32 / span full packets.  Each lane loads one 32-bit window of
+// its node's switches (span bits per packet, consecutive packets adjacent),
+// and lane L then assembles output word L with 32 / span shuffles: packet
+// L / span of the window, nodes (L % span) * 32 / span onwards.  Two loads
+// per lane replace the 2 * 32 / span loads per word of the block form.
+__global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
+    const LevelInfo& lv = plan->levels[level];
+    const LevelSide& ls = lv.side[side];
+    const GroupInfo& gi = plan->groups[side][ls.group];
+    const uint32_t rel = ls.rel;                 // >= 5
+    const uint32_t span_log2 = gi.depth - rel - 1; // < 5
+    const uint32_t span_mask = (1u << (1u << span_log2)) - 1u;
+    const uint32_t per_window_log2 = 5 - span_log2; // packets per lane window
+    const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint64_t windows = (full_packets + (1ull << per_window_log2) - 1) >> per_window_log2;
+    const uint64_t groups = 1ull << (level - 5);  // 32-node groups over all roots
+    const uint64_t total_warps = groups * windows;
+    const uint64_t section_bit = plan->section_offset[side] * 8;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t wi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total_warps;
+         wi += warps) {
+        const uint64_t group = wi / windows;
+        const uint64_t k0 = (wi - group * windows) << per_window_log2;
+        const uint32_t node = (uint32_t)(group << 5) + lane;
+        const uint64_t q = (uint64_t)node * pcap + (k0 << span_log2);
+        const uint64_t wq = q >> 5;
+        uint32_t window = __funnelshift_r(bits[wq], bits[wq + 1], (uint32_t)(q & 31));
+        // packets at or past full_packets belong to level_emit
+        const uint64_t valid = full_packets - k0; // > 0
+        if (valid < (1ull << per_window_log2)) {
+            window &= (1u << (uint32_t)(valid << span_log2)) - 1u;
+        }
+        const uint32_t p_local = lane >> span_log2;
+        const uint32_t g_out = lane & ((1u << span_log2) - 1u);
+        uint32_t v = 0;
+        for (uint32_t n = 0; n < (1u << per_window_log2); ++n) {
+            const uint32_t w = __shfl_sync(0xffffffffu, window,
+                (int)((g_out << per_window_log2) + n));
+            v |= ((w >> (p_local << span_log2)) & span_mask) << (n << span_log2);
+        }
+        const uint64_t packet = k0 + p_local;
+        if (v == 0 || packet >= full_packets) {
+            continue;
+        }
+        const uint32_t root_node = node & ~((1u << rel) - 1u);
+        const uint32_t n0 = (node & ((1u << rel) - 1u)) & ~31u; // first node of the group
+        const uint64_t dest = section_bit + switch_bit(addr[root_node], packet << span_log2) +
+            ((uint64_t)n0 << span_log2) + ((uint64_t)g_out << 5);
+        const uint32_t off = (uint32_t)(dest & 31);
+        atomicOr(blob + (dest >> 5), v << off);
+        if (off != 0 && (v >> (32 - off)) != 0) {
+            atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
+        }
+    }
+}
+
 // Word-wise form of level_emit for levels whose packets carry at least 32
 // switches of each node (span_log2 >= 5).  The switches of one node inside
 // one packet are a contiguous run of the node's bits and land on a

@@ -312,9 +312,22 @@ __device__ __forceinline__ U128 warp_factoradic_rank(uint32_t value, uint32_t co
     }
     const unsigned smaller = __shfl_sync(0xffffffffu, below, live ? value : 0);
     const uint32_t digit = live ? (uint32_t)__popc(smaller & ((1u << lane) - 1u)) : 0u;
-    U128 r = {digit, 0ull};
-    U128 m = {live ? (unsigned long long)(lane + 1) : 1ull, 0ull};
-    for (int d = 1; d < 32; d <<= 1) {
+    // The first three tree levels combine blocks of at most 8 radices, whose
+    // product stays below 25 * 26 * ... * 32 < 2^39: 64-bit arithmetic
+    // suffices there (and the partial rank is below the product).
+    unsigned long long r64 = digit;
+    unsigned long long m64 = live ? (unsigned long long)(lane + 1) : 1ull;
+    for (int d = 1; d < 8; d <<= 1) {
+        const unsigned long long r2 = __shfl_down_sync(0xffffffffu, r64, d);
+        const unsigned long long m2 = __shfl_down_sync(0xffffffffu, m64, d);
+        if ((lane & (2 * d - 1)) == 0) {
+            r64 = r64 * m2 + r2;
+            m64 *= m2;
+        }
+    }
+    U128 r = {r64, 0ull};
+    U128 m = {m64, 0ull};
+    for (int d = 8; d < 32; d <<= 1) {
         const U128 r2 = shfl_down128(r, d);
         const U128 m2 = shfl_down128(m, d);
         if ((lane & (2 * d - 1)) == 0) {

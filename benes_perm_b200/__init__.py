@@ -9,7 +9,8 @@ is no CPU fallback.  Errors raise the Python counterparts of the reference's
 exception types: ``ValueError`` for std::invalid_argument, ``OverflowError``
 for std::overflow_error, ``LengthError`` (a ``ValueError`` subclass, as
 std::length_error derives from std::logic_error) for std::length_error and
-``RuntimeError`` for std::runtime_error.
+``RuntimeError`` for std::runtime_error and ``IndexError`` for
+std::out_of_range (lookup verifier).
 """
 from __future__ import annotations
 
@@ -136,6 +137,13 @@ def library() -> ctypes.CDLL:
         lib.bpb200_probe_rank_bit.argtypes = [ctypes.c_uint64, fp, ctypes.c_uint32, ctypes.c_uint64,
                                               ctypes.POINTER(ctypes.c_int),
                                               ctypes.POINTER(ctypes.c_uint64)]
+        lib.bpb200_lookup_device.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                             fp, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_char_p,
+                                             ctypes.c_size_t]
+        lib.bpb200_probe_lookup.argtypes = [ctypes.c_uint64, fp, ctypes.c_char_p,
+                                            ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_uint64)]
         lib.bpb200_shutdown.restype = None
         lib.bpb200_set_profiling.argtypes = [ctypes.c_int]
         lib.bpb200_set_profiling.restype = None
@@ -160,6 +168,8 @@ def raise_for(code: int, message: str) -> None:
         raise OverflowError(message)
     if code == 3:
         raise LengthError(message)
+    if code == 5:
+        raise IndexError(message)
     raise RuntimeError(message or f"b200 backend error {code}")
 
 
@@ -473,6 +483,30 @@ def probe_rank_bit(count: int, fmt: FormatOptions, level: int, node: int):
                                          ctypes.byref(out))
     raise_for(rc, "not a leaf")
     return sec.value, out.value
+
+
+def lookup_device(d_blob: int, blob_len: int, count: int, fmt: Optional[FormatOptions],
+                  d_out: int, query_count: int, d_queries: Optional[int] = None,
+                  inverse: bool = False, stream: int = 0) -> None:
+    """Batch lookup verifier on a device blob: d_out[i] (uint64) = p[q] or,
+    with ``inverse``, p^-1[q], for q = d_queries[i] (uint64) or q = i when
+    ``d_queries`` is None.  Raises IndexError for a query >= count."""
+    cf = to_c_format(fmt)
+    err = ctypes.create_string_buffer(512)
+    rc = library().bpb200_lookup_device(d_blob, blob_len, count, ctypes.byref(cf), d_queries,
+                                        query_count, 1 if inverse else 0, d_out, stream, err, 512)
+    raise_for(rc, err.value.decode())
+
+
+def probe_lookup(count: int, fmt: Optional[FormatOptions], blob: bytes, value: int,
+                 inverse: bool = False) -> int:
+    """Host evaluation of the verifier's per-query walk (test hook)."""
+    cf = to_c_format(fmt)
+    out = ctypes.c_uint64(0)
+    rc = library().bpb200_probe_lookup(count, ctypes.byref(cf), blob, len(blob), value,
+                                       1 if inverse else 0, ctypes.byref(out))
+    raise_for(rc, "lookup failed")
+    return out.value
 
 
 def shutdown() -> None:

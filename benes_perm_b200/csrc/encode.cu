@@ -1118,3 +1118,6 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
 
 // File form: streamed file -> device -> file (compress_file).
 #include "file.inc"
+
+// Batch lookup verifier (device twin of the reference's lookup).
+#include "lookup.inc"

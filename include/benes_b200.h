@@ -23,6 +23,7 @@ extern "C" {
 #define BPB200_OVERFLOW 2         /* std::overflow_error (checked size arithmetic) */
 #define BPB200_LENGTH 3           /* std::length_error (does not fit) */
 #define BPB200_RUNTIME 4          /* std::runtime_error (CUDA or device status) */
+#define BPB200_OUT_OF_RANGE 5     /* std::out_of_range (lookup index >= size) */
 #define BPB200_UNAVAILABLE 6      /* std::runtime_error("b200 backend is unavailable") */
 
 /* benes::FormatOptions (include/benes/benes.hpp:32-39).  A cluster count of
@@ -217,6 +218,25 @@ int bpb200_probe_switch_bit(uint64_t count, const bpb200_format* format, int sid
     uint32_t level, uint64_t node, uint64_t pair, uint64_t* bit);
 int bpb200_probe_rank_bit(uint64_t count, const bpb200_format* format, uint32_t level,
     uint64_t node, int* section, uint64_t* bit);
+
+/* Batch lookup verifier: a read-only device twin of the reference's lookup
+ * (src/internal.hpp:1035-1124, behind CompressedPermutationView::forward /
+ * inverse), for checking every entry of blobs too large to re-encode on the
+ * host.  The library's own lookup is not replaced.  For each i <
+ * query_count, d_out[i] = p[q] (inverse = 0) or p^-1[q] (inverse != 0),
+ * q = d_queries[i], or q = i when d_queries is NULL; p is the permutation
+ * of `count` entries encoded in the device blob of blob_len bytes with
+ * `format`.  Queued on `stream`; returns after it completes.  A query >=
+ * count returns BPB200_OUT_OF_RANGE ("permutation lookup is out of range",
+ * std::out_of_range in the reference) with that entry set to UINT64_MAX. */
+int bpb200_lookup_device(const void* d_blob, uint64_t blob_len, uint64_t count,
+    const bpb200_format* format, const uint64_t* d_queries, uint64_t query_count, int inverse,
+    uint64_t* d_out, void* stream, char* err, size_t err_len);
+
+/* Host evaluation of the verifier's per-query walk (test hook, no device
+ * work): one forward or inverse lookup in a host blob. */
+int bpb200_probe_lookup(uint64_t count, const bpb200_format* format, const uint8_t* blob,
+    uint64_t blob_len, uint64_t value, int inverse, uint64_t* out);
 
 #ifdef __cplusplus
 }

@@ -197,6 +197,63 @@ def test_config_4_sattolo_100m(gpu, reference):
     assert blob == want
 
 
+def _device_round_trip(gpu, blob, perm, fmt):
+    """Every forward and inverse lookup of `blob` through the device verifier
+    (bpb200_lookup_device): p[i] for all i, then p^-1[p[i]] == i."""
+    import torch
+    n = len(perm)
+    d_blob = torch.frombuffer(bytearray(blob), dtype=torch.uint8).cuda()
+    d_perm = torch.from_numpy(np.ascontiguousarray(perm, dtype=np.uint64).view(np.int64)).cuda()
+    out = torch.empty(n, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    gpu.lookup_device(d_blob.data_ptr(), len(blob), n, fmt, out.data_ptr(), n, stream=stream)
+    assert torch.equal(out, d_perm)
+    gpu.lookup_device(d_blob.data_ptr(), len(blob), n, fmt, out.data_ptr(), n,
+                      d_queries=d_perm.data_ptr(), inverse=True, stream=stream)
+    assert torch.equal(out, torch.arange(n, dtype=torch.int64, device="cuda"))
+
+
+def test_lookup_verifier_round_trips(gpu, oracle):
+    cases = [(1 << 16, {}, gpu.PermutationKind.uniform),
+             (1 << 20, dict(middle_group_log2=5, input_clusters=[8, 7], output_clusters=[7, 8],
+                            middle_placement=1), gpu.PermutationKind.bit_reversal),
+             (1_000_003, dict(middle_group_log2=4, middle_placement=2),
+              gpu.PermutationKind.single_cycle),
+             (4097, dict(middle_group_log2=1, middle_placement=0), gpu.PermutationKind.identity)]
+    for n, kw, kind in cases:
+        perm = gpu.fill_permutation(kind, 6, n)
+        fmt = b200_format(gpu, kw)
+        blob = gpu.compress(perm, gpu.CompressOptions(format=fmt))
+        _device_round_trip(gpu, blob, perm, fmt)
+
+
+def test_lookup_verifier_agrees_with_oracle_and_errors(gpu, oracle):
+    import torch
+    n = 50_000
+    kw = dict(middle_group_log2=3, middle_placement=1, input_clusters=[4, 9])
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 8, n)
+    blob = oracle.compress(perm, oracle_format(kw))
+    fmt = b200_format(gpu, kw)
+    queries = np.random.default_rng(2).integers(0, n, 512).astype(np.int64)
+    d_blob = torch.frombuffer(bytearray(blob), dtype=torch.uint8).cuda()
+    d_q = torch.from_numpy(queries).cuda()
+    out = torch.empty(512, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    for inverse in (False, True):
+        gpu.lookup_device(d_blob.data_ptr(), len(blob), n, fmt, out.data_ptr(), 512,
+                          d_queries=d_q.data_ptr(), inverse=inverse, stream=stream)
+        want = [oracle.lookup(blob, int(q), inverse=inverse) for q in queries]
+        assert out.cpu().tolist() == want
+    d_q[7] = n
+    with pytest.raises(IndexError):
+        gpu.lookup_device(d_blob.data_ptr(), len(blob), n, fmt, out.data_ptr(), 512,
+                          d_queries=d_q.data_ptr(), stream=stream)
+    assert int(out[7]) == -1 and int(out[6]) == int(perm[int(queries[6])])
+    with pytest.raises(ValueError):
+        gpu.lookup_device(d_blob.data_ptr(), len(blob) - 1, n, fmt, out.data_ptr(), 512,
+                          stream=stream)
+
+
 @pytest.mark.slow
 def test_config_3_uniform_2p30_lookups(gpu, oracle):
     n = 1 << 30
@@ -205,3 +262,5 @@ def test_config_3_uniform_2p30_lookups(gpu, oracle):
     blob = gpu.compress(perm, gpu.CompressOptions(format=fmt))
     assert len(blob) == 3850371096
     _spot_check(oracle, blob, perm, count=256, seed=3)
+    # every entry, both directions, on the device
+    _device_round_trip(gpu, blob, perm, fmt)

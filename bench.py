@@ -15,7 +15,10 @@ point), timed with CUDA events on the launching stream over exactly K steps,
 max over ranks.  ``e2e``: the same metric through the host entry point,
 including the host->device copy of the input from pinned memory and the
 device->host copy of the blob.  The path does not shard: with N GPUs every
-rank compresses its own permutation (replicas, weak scaling).
+rank compresses its own permutation (replicas, weak scaling).  After the
+timed regions every entry of the measured blob is checked in both
+directions through the device lookup verifier and the host entry point's
+blob is compared with the device one (``verified``); a failed check exits 1.
 ``--impl reference`` times the reference's portable_cpu encoder (built from
 its own sources into oracle/_ref) on the host cores instead.
 """
@@ -352,9 +355,15 @@ def b200_arm(args, world, rank, local):
     e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, f"cuda:{local}")
     e2e_value = replica_throughput(n, args.e2e_steps, world, e2e_secs)
 
+    verified = verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream)
+    if not verified["ok"]:
+        print(f"rank {rank}: the measured blob failed verification: {verified}",
+              file=sys.stderr, flush=True)
     if rank != 0:
         if dist is not None:
             dist.destroy_process_group()
+        if not verified["ok"]:
+            sys.exit(1)
         return
 
     # roofline of the dominant kernel kind: its algorithmic bytes over all of
@@ -403,12 +412,36 @@ def b200_arm(args, world, rank, local):
         "kernel_seconds": {k: round(v, 6) for k, v in kernel_secs.items()},
         "kernel_launches": kernel_counts,
         "levels": {"depth": depth, "tile_level": tile, "walk_levels": sorted(walk_levels)},
+        "verified": verified,
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(world)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    if not verified["ok"]:
+        sys.exit(1)
+
+
+def verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream):
+    """Checks the measured output after the timed regions: every entry of the
+    device blob round-trips through the device lookup verifier (p[i] for all
+    i, then p^-1[p[i]] == i), and the host entry point's blob equals the
+    device-resident one byte for byte."""
+    t0 = time.perf_counter()
+    out = torch.empty(n, dtype=torch.int64, device=d_in.device)
+    bp.lookup_device(d_blob.data_ptr(), size, n, fmt, out.data_ptr(), n,
+                     stream=stream.cuda_stream)
+    forward = bool(torch.equal(out, d_in))
+    bp.lookup_device(d_blob.data_ptr(), size, n, fmt, out.data_ptr(), n,
+                     d_queries=d_in.data_ptr(), inverse=True, stream=stream.cuda_stream)
+    inverse = bool(torch.equal(out, torch.arange(n, dtype=torch.int64, device=d_in.device)))
+    del out
+    same = bool(torch.equal(host_blob.to(d_blob.device), d_blob[:size]))
+    return {"ok": forward and inverse and same, "forward_lookups": forward,
+            "inverse_lookups": inverse, "host_blob_equals_device_blob": same,
+            "method": "every entry through bpb200_lookup_device, both directions",
+            "seconds": round(time.perf_counter() - t0, 3)}
 
 
 def _section_bits(n, fmt):

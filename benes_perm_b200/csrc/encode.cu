@@ -565,6 +565,23 @@ Format to_format(const bpb200_format* f) {
     return out;
 }
 
+// Device buffers must be aligned to the width the kernels access them with
+// (4-byte blob words, entry-width input values); a misaligned pointer would
+// fault on the device, so it is rejected here.
+int check_device_buffers(const void* d_entries, uint32_t entry_bytes, const void* d_blob,
+    char* err, size_t err_len) {
+    if (((uintptr_t)d_blob & 3u) != 0) {
+        set_error(err, err_len, "device blob must be 4-byte aligned");
+        return kInvalidArgument;
+    }
+    if ((entry_bytes == 4 || entry_bytes == 8) &&
+        ((uintptr_t)d_entries & (uintptr_t)(entry_bytes - 1)) != 0) {
+        set_error(err, err_len, "device input must be aligned to its entry width");
+        return kInvalidArgument;
+    }
+    return kOk;
+}
+
 // Validation shared by both entry points; fills the layout and plan.
 int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
     uint64_t blob_len, Workspace& w, Call* call, char* err, size_t err_len) {
@@ -835,9 +852,8 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
             set_error(err, err_len, "b200 backend is unavailable");
             return kUnavailable;
         }
-        if (((uintptr_t)d_blob & 3u) != 0) {
-            set_error(err, err_len, "device blob must be 4-byte aligned");
-            return kInvalidArgument;
+        if (const int bad = check_device_buffers(d_entries, entry_bytes, d_blob, err, err_len)) {
+            return bad;
         }
         Lease lease(device);
         Workspace& w = *lease.w;
@@ -1028,9 +1044,8 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
                 "the allocation-free entry point accepts at most 262144 (2^18) entries");
             return kLength;
         }
-        if (((uintptr_t)d_blob & 3u) != 0) {
-            set_error(err, err_len, "device blob must be 4-byte aligned");
-            return kInvalidArgument;
+        if (const int bad = check_device_buffers(d_entries, entry_bytes, d_blob, err, err_len)) {
+            return bad;
         }
         // One host thread at a time stages the plan; device-side overlap of
         // two calls is the caller's to avoid (they would share the scratch).

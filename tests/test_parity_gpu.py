@@ -158,6 +158,24 @@ def test_device_entry_point(gpu, oracle):
                                                                 middle_placement=2)))
 
 
+def test_misaligned_device_buffers_are_rejected(gpu):
+    # rejected on the host before any device work; a valid call still works
+    import torch
+    n = 1000
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 1, n, np.uint64)
+    size = gpu.encoded_size(n)
+    d_in = torch.from_numpy(perm.view(np.int64)).cuda()
+    raw = torch.zeros(size + 16, dtype=torch.uint8, device="cuda")
+    with pytest.raises(ValueError, match="entry width"):
+        gpu.compress_device(d_in.data_ptr() + 4, n, 8, raw.data_ptr(), size)
+    with pytest.raises(ValueError, match="4-byte aligned"):
+        gpu.compress_device(d_in.data_ptr(), n, 8, raw.data_ptr() + 1, size)
+    with pytest.raises(ValueError, match="entry width"):
+        gpu.compress_batch_device([(d_in.data_ptr() + 4, n, 8, None, raw.data_ptr(), size)])
+    gpu.compress_device(d_in.data_ptr(), n, 8, raw.data_ptr(), size)
+    assert raw[:size].cpu().numpy().tobytes() == gpu.compress(perm)
+
+
 def _spot_check(oracle, blob, perm, count=1024, seed=0):
     oracle.validate(blob)
     rng = np.random.default_rng(seed)

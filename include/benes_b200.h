@@ -68,8 +68,10 @@ int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
 /* Device-resident form of bpb200_compress (no reference counterpart; the
  * reference copies host spans, src/cuda/benes_cuda.cu:1397-1409).
  * `d_entries` and `d_blob` are device pointers on the current device;
- * `d_blob` must be 4-byte aligned with room for blob_len rounded up to a
- * multiple of 4 bytes.  Work is queued on `stream` (a cudaStream_t, NULL for
+ * `d_entries` must be aligned to entry_bytes and `d_blob` 4-byte aligned
+ * with room for blob_len rounded up to a multiple of 4 bytes (misaligned
+ * pointers return BPB200_INVALID_ARGUMENT before any device work; the same
+ * holds for the batched form).  Work is queued on `stream` (a cudaStream_t, NULL for
  * the legacy default stream); the call returns after the work completes and
  * the device status word has been checked. */
 int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry_bytes,

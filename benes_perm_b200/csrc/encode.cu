@@ -402,19 +402,26 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             ++rounds;
         }
         uint4* sstate[2] = {w.state[1], w.state[1] + supers};
+        // few super-rulers: every round in one CTA; otherwise one launch pair per round
+        const bool one_block = supers <= kJumpBlockMaxStates;
         rec.launch(kKindJump, [&] {
             check(cudaMemsetAsync(w.super_of, 0xff, (uint64_t)buckets * 4, st),
                 "cudaMemsetAsync(super rulers)");
             ruler_super_walk<<<grid_for(supers, kLevelThreads), kLevelThreads, 0, st>>>(
                 w.state[0], buckets, sstate[0], w.super_of, ctl);
             ruler_super_short<<<gw, kLevelThreads, 0, st>>>(w.state[0], buckets, w.super_of, ctl);
+            if (one_block) {
+                ruler_jump_block<<<1, kJumpBlockThreads, 0, st>>>(sstate[0], sstate[1], supers,
+                    rounds, ctl);
+                return;
+            }
             const int gj = grid_for(supers, kLevelThreads);
             for (uint32_t r = 0; r <= rounds; ++r) {
                 ruler_jump<<<gj, kLevelThreads, 0, st>>>(sstate[r & 1], sstate[(r + 1) & 1],
                     supers, r, ctl);
                 ruler_check<<<1, 1, 0, st>>>(r, ctl);
             }
-        }, 2 + 2 * (rounds + 1));
+        }, one_block ? 3 : 2 + 2 * (rounds + 1));
     }
     rec.launch(kKindUnion, [&] {
         level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard,

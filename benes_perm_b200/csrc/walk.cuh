@@ -336,6 +336,98 @@ __global__ void ruler_check(uint32_t round, uint32_t* control) {
     control[kCtlChanged] = 0;
 }
 
+// Levels with few super-rulers spend their jumping time on launches, not on
+// the rounds: a round over a few thousand states is shorter than the gap
+// between two launches.  ruler_jump_block runs all rounds of such a level in
+// one CTA, a block barrier between rounds, and leaves the control words as
+// the ruler_jump / ruler_check sequence would (kCtlFinal names the buffer
+// the last executed round wrote; kCtlDone is set when a round changed
+// nothing).  Each thread handles kJumpBlockBatch states at a time, loading
+// all of them before their successors so the gathers overlap.
+constexpr uint32_t kJumpBlockThreads = 1024;
+constexpr uint32_t kJumpBlockBatch = 4;
+#ifndef BPB200_JUMP_BLOCK_LOG2
+#define BPB200_JUMP_BLOCK_LOG2 14
+#endif
+constexpr uint32_t kJumpBlockMaxStates = 1u << BPB200_JUMP_BLOCK_LOG2;
+
+__global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* s0, uint4* s1,
+    uint32_t supers, uint32_t rounds, uint32_t* control) {
+    // written by earlier launches: every thread reads the same values
+    if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
+        *(volatile uint32_t*)(control + kCtlHard) != 0) {
+        return;
+    }
+    __shared__ uint32_t changed[2];
+    if (threadIdx.x == 0) {
+        changed[0] = 0u;
+        changed[1] = 0u;
+    }
+    __syncthreads();
+    uint32_t final_buffer = 0;
+    bool done = false;
+    bool bad = false;
+    for (uint32_t r = 0; r <= rounds; ++r) {
+        const uint4* src = (r & 1u) ? s1 : s0;
+        uint4* dst = (r & 1u) ? s0 : s1;
+        bool ch = false;
+        for (uint32_t base = 0; base < supers; base += kJumpBlockThreads * kJumpBlockBatch) {
+            uint4 me[kJumpBlockBatch], nx[kJumpBlockBatch];
+#pragma unroll
+            for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
+                const uint32_t i = base + k * kJumpBlockThreads + threadIdx.x;
+                me[k] = i < supers ? __ldcg(src + i) : make_uint4(kNoRuler, 0u, 0u, 0u);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
+                const bool live = me[k].x != kNoRuler && me[k].x < supers;
+                bad |= me[k].x != kNoRuler && me[k].x >= supers;
+                nx[k] = live ? __ldcg(src + me[k].x) : me[k];
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
+                const uint32_t i = base + k * kJumpBlockThreads + threadIdx.x;
+                if (i >= supers) {
+                    continue;
+                }
+                if (me[k].x == kNoRuler || me[k].x >= supers) {
+                    dst[i] = me[k];
+                    continue;
+                }
+                const uint4 out = make_uint4(nx[k].x, min(me[k].y, nx[k].y),
+                    min(me[k].z, nx[k].z), 0u);
+                ch |= (out.y != me[k].y) || (out.z != me[k].z);
+                dst[i] = out;
+            }
+        }
+        if (ch) {
+            changed[r & 1u] = 1u;
+        }
+        __syncthreads(); // this round's states and flag are visible to the block
+        const bool any = changed[r & 1u] != 0u;
+        final_buffer = (r + 1u) & 1u;
+        if (threadIdx.x == 0) {
+            changed[(r + 1u) & 1u] = 0u; // every thread read it a round ago
+        }
+        __syncthreads();
+        if (!any) {
+            done = true;
+            break;
+        }
+    }
+    if (bad) {
+        atomicOr(control + kCtlHard, 1u); // a successor out of range: fall back to union-find
+    }
+    if (threadIdx.x == 0) {
+        control[kCtlFinal] = final_buffer;
+        if (done) {
+            control[kCtlDone] = 1u;
+        }
+        control[kCtlChanged] = 0u;
+        control[kCtlClaimJump] = 0u;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Super-rulers.  Jumping over all rulers costs a full pass over their states
 // per round (about log2 of the rulers in an orbit rounds).  Instead every

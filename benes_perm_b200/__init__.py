@@ -232,6 +232,8 @@ def compress(permutation, options: Optional[CompressOptions] = None,
     arr = np.ascontiguousarray(permutation)
     if arr.dtype not in (np.uint32, np.uint64):
         raise TypeError("permutation must be uint32 or uint64")
+    if arr.ndim != 1:
+        raise ValueError("permutation must be a one-dimensional array")
     n = int(arr.size)
     cf = to_c_format(options.format)
     err = ctypes.create_string_buffer(512)
@@ -414,6 +416,8 @@ class Server:
         arr = np.ascontiguousarray(permutation)
         if arr.dtype not in (np.uint32, np.uint64):
             raise TypeError("permutation must be uint32 or uint64")
+        if arr.ndim != 1:
+            raise ValueError("permutation must be a one-dimensional array")
         n = int(arr.size)
         if n == 0:
             raise ValueError("permutation size is out of range")

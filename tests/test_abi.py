@@ -137,3 +137,17 @@ def test_compress_without_gpu_reports_unavailable(b200):
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError):
         b200.compress(np.arange(10, dtype=np.uint32))
+
+
+def test_python_argument_errors_come_before_device_work(b200):
+    # the reference takes a span of uint32 or uint64; an empty one is
+    # "permutation size is out of range" (src/benes.cpp:153-156)
+    with pytest.raises(TypeError):
+        b200.compress(np.arange(10, dtype=np.int64))
+    with pytest.raises(ValueError, match="one-dimensional"):
+        b200.compress(np.arange(16, dtype=np.uint32).reshape(4, 4))
+    with pytest.raises(ValueError, match="out of range"):
+        b200.compress(np.zeros(0, dtype=np.uint64))
+    with pytest.raises(ValueError, match="middle_group_log2"):
+        b200.compress(np.arange(10, dtype=np.uint32),
+                      b200.CompressOptions(format=b200.FormatOptions(middle_group_log2=9)))

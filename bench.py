@@ -40,7 +40,25 @@ sys.path.insert(0, ROOT)
 METRIC = "entries/sec compressed bit-exact at N=2^30; serving p50/p99 latency vs plain"
 UNIT = "entries/s"
 SEED = 0x5EED_2030
+STREAM_TEST_SEED = 0x5EED_0240   # the mixed stream the GPU tests replay
 CPU_SAMPLE_N = 1 << 23
+
+
+def serving_specs(requests, max_log2, seed):
+    """The mixed-size request stream: per request (N, generator kind, dtype,
+    middle_group_log2, placement), N = round(2^U(10, max_log2)), Fisher-Yates
+    or Sattolo, uint32 or uint64, m in {4, 5}, placement uniform over the
+    three, default clusters.  Request i's permutation uses seed + i."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for _ in range(requests):
+        n = int(round(2 ** rng.uniform(10, max_log2)))
+        kind = int(rng.integers(0, 2))                   # Fisher-Yates or Sattolo
+        dtype = np.uint32 if rng.integers(0, 2) == 0 else np.uint64
+        m = int(rng.choice([4, 5]))
+        placement = int(rng.integers(0, 3))
+        specs.append((n, kind, dtype, m, placement))
+    return specs
 
 
 def parse_args():
@@ -477,15 +495,8 @@ def serving_arm(args):
 
     import benes_perm_b200 as bp
 
-    rng = np.random.default_rng(SEED)
-    specs = []
-    for i in range(args.requests):
-        n = int(round(2 ** rng.uniform(10, args.max_log2)))
-        kind = int(rng.integers(0, 2))                   # Fisher-Yates or Sattolo
-        dtype = np.uint32 if rng.integers(0, 2) == 0 else np.uint64
-        m = int(rng.choice([4, 5]))
-        placement = int(rng.integers(0, 3))
-        specs.append((n, kind, dtype, m, placement))
+    specs = serving_specs(args.requests, args.max_log2, SEED)
+    rng = np.random.default_rng(SEED + 1)                # arrival times
     opts = [bp.CompressOptions(format=bp.FormatOptions(middle_group_log2=m,
                                                        middle_placement=bp.MiddlePlacement(pl)))
             for (_, _, _, m, pl) in specs]

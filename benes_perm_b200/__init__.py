@@ -278,7 +278,7 @@ def compress_file(input, output, input_width: InputValueWidth = InputValueWidth.
 
 
 KERNEL_KINDS = ("prologue", "inverse", "descriptors", "union", "orient", "resolve",
-                "output_bits", "tile", "emit", "walk", "jump")
+                "output_bits", "tile", "emit", "walk", "jump", "place")
 
 
 def set_profiling(enabled: bool) -> None:

@@ -46,6 +46,7 @@ enum KernelKind : int {
     kKindEmit,
     kKindWalk,
     kKindJump,
+    kKindPlace, // partitioned inverse (level_bucket + level_place)
     kKernelKinds
 };
 
@@ -365,7 +366,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
         check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
         const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kBucketThreads);
-        rec.launch(kKindInverse, [&] {
+        rec.launch(kKindPlace, [&] {
             level_bucket<TV><<<gb, kBucketThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
                 w.d_status);
             level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
@@ -976,11 +977,10 @@ int bpb200_probe_rank_bit(uint64_t count, const bpb200_format* format, uint32_t 
 // ---------------------------------------------------------------------------
 // Allocation-free entry point.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA stream is
-// being captured into a graph (allocation is not allowed during capture),
-// processes whose device memory is owned by a pooling allocator that must
-// account for every byte, and latency-critical paths that cannot afford the
-// device-wide synchronisation cudaMalloc/cudaFree can imply.  For them,
+// Some callers cannot call cudaMalloc: processes whose device memory is
+// owned by a pooling allocator that must account for every byte, and
+// latency-critical paths that cannot afford the device-wide synchronisation
+// cudaMalloc/cudaFree can imply.  For them,
 // bpb200_compress_device_noalloc runs the same encode with all of its
 // scratch (plan, status word, level arrays, inverse, union-find words,
 // colour bits, node descriptors) carved out of one file-scope device array
@@ -1059,7 +1059,7 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         std::lock_guard<std::mutex> lock(noalloc::g_mutex);
         if (noalloc::g_scratch[device] == nullptr) {
             // first call on this device: resolve the array's device address
-            // (must happen before any stream capture that uses this entry point)
+            // (callers make this first call before capturing any stream)
             void* ptr = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&ptr, bpb200_noalloc_scratch);
             if (e != cudaSuccess || ptr == nullptr) {

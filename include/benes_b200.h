@@ -4,8 +4,9 @@
  *
  * Every entry point is plain C: pointers, sizes and status codes, no C++ or
  * torch types.  The reference library binds these from a thin C++ shim that
- * plugs in beside its other accelerated backends; the
- * status codes map one-to-one onto the exception types the reference throws.
+ * plugs in beside its other accelerated backends (src/internal.hpp:1190-1197,
+ * src/backends_stub.cpp:25-40); the status codes map one-to-one onto the
+ * exception types the reference throws.
  */
 #ifndef BENES_B200_H
 #define BENES_B200_H
@@ -80,18 +81,20 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
 
 /* Allocation-free form of bpb200_compress_device.  No counterpart in the
  * reference: its backends all allocate per call.  For callers that cannot
- * call cudaMalloc — code that runs while a stream is being captured into a
- * CUDA graph, processes whose device memory belongs to a pooling allocator,
- * latency-critical paths that must not trigger the synchronisation an
- * allocation can imply.  Same arguments and result bytes as
- * bpb200_compress_device (device input and blob, work queued on `stream`),
- * but every byte of scratch comes from one fixed device array inside this
- * library (under 7 MB, present on every GPU that loads the library until
- * the process exits), so it accepts at most 262144 (2^18) entries and
- * returns BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.
- * The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before capturing a stream
- * that uses this entry point.  All calls share the one array: calls whose
+ * call cudaMalloc: processes whose device memory belongs to a pooling
+ * allocator that must account for every byte, and latency-critical paths
+ * that must not pay for the device-wide synchronisation cudaMalloc/cudaFree
+ * can imply.  Same arguments and result bytes as bpb200_compress_device
+ * (device input and blob, work queued on `stream`), but every byte of
+ * scratch comes from one fixed device array inside this library (under
+ * 7 MB, present on every GPU that loads the library until the process
+ * exits), so it accepts at most 262144 (2^18) entries and returns
+ * BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.  Like
+ * bpb200_compress_device, each call uploads its plan from host memory,
+ * waits for `stream` to finish the work and reads the device status word
+ * back before it returns.  The first call on each device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call
+ * before capturing any stream.  All calls share the one array: calls whose
  * GPU work overlaps (different streams or host threads without ordering)
  * race and corrupt each other's results.  Each call clears what it needs
  * cleared (blob, status word, validation sentinels). */
@@ -108,7 +111,8 @@ int bpb200_compress_device_noalloc(const void* d_entries, uint64_t count,
  * blob streamed back the same way.  Errors, in the reference's order:
  * RUNTIME "cannot open permutation input file"; INVALID_ARGUMENT
  * "permutation input has an invalid element width or size" (width not 4/8,
- * empty file, size not a multiple of the width); UNAVAILABLE without a
+ * empty file, size not a multiple of the width, not a regular file);
+ * UNAVAILABLE without a
  * usable GPU; RUNTIME "failed to read permutation input file"; then every
  * error of bpb200_compress; RUNTIME "failed to write compressed permutation
  * file".  The output file is created only after the encode succeeded. */
@@ -189,8 +193,8 @@ void bpb200_shutdown(void);
  * of later calls is bracketed by CUDA events.  bpb200_last_profile reports,
  * for the calling thread's last call, seconds and launch counts per kernel
  * kind (0 prologue, 1 inverse, 2 descriptors, 3 union, 4 orient, 5 resolve,
- * 6 output bits, 7 tile, 8 emit) and the total number of kernel launches; it returns
- * the number of kinds. */
+ * 6 output bits, 7 tile, 8 emit, 9 walk, 10 jump, 11 partitioned inverse)
+ * and the total number of kernel launches; it returns the number of kinds. */
 void bpb200_set_profiling(int enabled);
 
 /* Test hook: nonzero makes later calls colour every global level with the

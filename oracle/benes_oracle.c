@@ -948,3 +948,110 @@ int oracle_lookup(const uint8_t* blob, uint64_t blob_len, uint64_t value,
     *result = index;
     return ORACLE_OK;
 }
+
+/* --------------------------------------------------------- workload inputs
+ *
+ * The configs' seeded permutations, restated here so that the CPU baseline
+ * and the fixture generators need nothing from the B200 library.  Not part
+ * of the reference (its tests shuffle with std::shuffle,
+ * tests/test_benes.cpp:60-68); the configs name the published generators:
+ * xoshiro256** (Blackman and Vigna, 2018) whose four state words are
+ * successive splitmix64 outputs from the seed, bounded draws in [0, range)
+ * by Lemire's multiply-shift with rejection (2019), and shuffles from the
+ * top index down: Fisher-Yates draws j in [0, i], Sattolo j in [0, i - 1]
+ * (one n-cycle).  Kinds: 0 Fisher-Yates, 1 Sattolo, 2 identity, 3 reverse,
+ * 4 bit reversal (power-of-two counts only). */
+
+typedef struct {
+    uint64_t s[4];
+} xoshiro_t;
+
+static uint64_t splitmix_next(uint64_t* x) {
+    uint64_t z = (*x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+static uint64_t rotate_left(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+
+static uint64_t xoshiro_next(xoshiro_t* g) {
+    uint64_t* s = g->s;
+    const uint64_t result = rotate_left(s[1] * 5, 7) * 9;
+    const uint64_t t = s[1] << 17;
+    s[2] ^= s[0];
+    s[3] ^= s[1];
+    s[1] ^= s[2];
+    s[0] ^= s[3];
+    s[2] ^= t;
+    s[3] = rotate_left(s[3], 45);
+    return result;
+}
+
+static uint64_t xoshiro_below(xoshiro_t* g, uint64_t range) {
+    u128 m = (u128)xoshiro_next(g) * range;
+    if ((uint64_t)m < range) {
+        const uint64_t threshold = (0 - range) % range;
+        while ((uint64_t)m < threshold) {
+            m = (u128)xoshiro_next(g) * range;
+        }
+    }
+    return (uint64_t)(m >> 64);
+}
+
+#define ORACLE_SHUFFLE(T)                                                          \
+    static void shuffle_##T(T* a, uint64_t n, uint64_t seed, int cycle) {          \
+        for (uint64_t i = 0; i < n; ++i) a[i] = (T)i;                              \
+        if (n < 2) return;                                                         \
+        xoshiro_t g;                                                               \
+        uint64_t x = seed;                                                         \
+        for (int k = 0; k < 4; ++k) g.s[k] = splitmix_next(&x);                    \
+        /* draws do not depend on the array: draw a block ahead and prefetch */  \
+        uint64_t draw[32];                                                         \
+        for (uint64_t top = n - 1; top >= 1;) {                                    \
+            const uint64_t steps = top < 32 ? top : 32;                            \
+            for (uint64_t t = 0; t < steps; ++t) {                                 \
+                draw[t] = xoshiro_below(&g, cycle ? top - t : top - t + 1);        \
+                __builtin_prefetch(a + draw[t], 1, 0);                             \
+            }                                                                      \
+            for (uint64_t t = 0; t < steps; ++t) {                                 \
+                const T keep = a[top - t];                                         \
+                a[top - t] = a[draw[t]];                                           \
+                a[draw[t]] = keep;                                                 \
+            }                                                                      \
+            top -= steps;                                                          \
+        }                                                                          \
+    }
+ORACLE_SHUFFLE(uint32_t)
+ORACLE_SHUFFLE(uint64_t)
+
+int oracle_fill_permutation(uint32_t kind, uint64_t seed, uint64_t count,
+    uint32_t entry_bytes, void* out) {
+    if (entry_bytes != 4 && entry_bytes != 8) return ORACLE_INVALID_ARGUMENT;
+    if (entry_bytes == 4 && count > 0x100000000ull) return ORACLE_INVALID_ARGUMENT;
+    if (kind == 4 && (count == 0 || (count & (count - 1)) != 0)) return ORACLE_INVALID_ARGUMENT;
+    if (kind > 4) return ORACLE_INVALID_ARGUMENT;
+    uint32_t* a32 = (uint32_t*)out;
+    uint64_t* a64 = (uint64_t*)out;
+    if (kind <= 1) {
+        if (entry_bytes == 4) {
+            shuffle_uint32_t(a32, count, seed, (int)kind);
+        } else {
+            shuffle_uint64_t(a64, count, seed, (int)kind);
+        }
+        return ORACLE_OK;
+    }
+    uint32_t bits = 0;
+    while (kind == 4 && (1ull << bits) < count) ++bits;
+    for (uint64_t i = 0; i < count; ++i) {
+        uint64_t v = i;
+        if (kind == 3) {
+            v = count - 1 - i;
+        } else if (kind == 4) {
+            v = 0;
+            for (uint32_t b = 0; b < bits; ++b) v |= ((i >> b) & 1ull) << (bits - 1 - b);
+        }
+        if (entry_bytes == 4) a32[i] = (uint32_t)v; else a64[i] = v;
+    }
+    return ORACLE_OK;
+}

@@ -84,6 +84,13 @@ int oracle_middle_bit(uint64_t count, const oracle_format* format,
 /* factoradic_bit_count (src/internal.hpp:173-183). */
 uint32_t oracle_factoradic_bits(uint32_t size);
 
+/* Seeded workload permutations of the benchmark configs (not part of the
+ * reference): kind 0 Fisher-Yates, 1 Sattolo single cycle, 2 identity,
+ * 3 reverse, 4 bit reversal.  xoshiro256** seeded by splitmix64(seed),
+ * Lemire bounded draws.  `out` holds count values of entry_bytes (4 or 8). */
+int oracle_fill_permutation(uint32_t kind, uint64_t seed, uint64_t count,
+    uint32_t entry_bytes, void* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,8 +16,12 @@ from typing import Optional, Sequence
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbenes_ref.so")
+SHIM_DRIVER = os.path.join(HERE, "_ref", "shim", "driver")
+# where the reference sources lie (only the build recipes read them)
+REF_DIR = os.environ.get("BENES_REFERENCE_DIR", "/root/reference")
 
 
 class CFormat(ctypes.Structure):
@@ -53,10 +57,58 @@ class CheckerError(Exception):
 
 
 def build() -> None:
-    """Builds liboracle.so, and the reference library when its sources exist."""
+    """Builds liboracle.so and, when the reference sources exist, the
+    reference library and the integration-shim driver."""
     subprocess.run(["make", "-s", "liboracle.so"], cwd=HERE, check=True)
-    if os.path.exists("/root/reference/src/benes.cpp"):
-        subprocess.run(["make", "-s", "ref"], cwd=HERE, check=True)
+    if os.path.exists(os.path.join(REF_DIR, "src", "benes.cpp")):
+        subprocess.run(["make", "-s", "ref", f"REF={REF_DIR}"], cwd=HERE, check=True)
+        build_shim()
+
+
+def integration_blocks():
+    """The C++ of the integration notes: the backend unit and its
+    declarations (section 2) and the dispatch fragment (section 3)."""
+    import re
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    section2 = text.split("## 2.", 1)[1].split("\n## 3.", 1)[0]
+    section3 = text.split("## 3.", 1)[1].split("\n## 4.", 1)[0]
+    blocks = re.findall(r"```cpp\n(.*?)```", section2, re.S)
+    if len(blocks) != 2:
+        raise ValueError("section 2 must hold the backend unit and its declarations")
+    unit = next(b for b in blocks if "#include <benes_b200.h>" in b)
+    decls = next(b for b in blocks if b is not unit)
+    dispatch = re.findall(r"```cpp\n(.*?)```", section3, re.S)[0]
+    return unit, decls, dispatch
+
+
+def build_shim() -> str:
+    """Compiles the integration notes' shim, as written there, with
+    oracle/shim_driver.cpp against the reference's headers, the reference
+    library (oracle/_ref) and libbenes_b200.so, into oracle/_ref/shim/driver.
+    The reference headers lack the appended Backend::b200 enumerator, so the
+    dispatch fragment names it as the driver's kB200 constant."""
+    work = os.path.dirname(SHIM_DRIVER)
+    os.makedirs(work, exist_ok=True)
+    unit, decls, dispatch = integration_blocks()
+    with open(os.path.join(work, "b200_decls.hpp"), "w") as f:
+        f.write('#pragma once\n#include "internal.hpp"\n' + decls)
+    with open(os.path.join(work, "benes_b200_backend.cpp"), "w") as f:
+        f.write('#include "b200_decls.hpp"\n' + unit)
+    with open(os.path.join(work, "dispatch_fragment.inc"), "w") as f:
+        f.write(dispatch.replace("Backend::b200", "kB200"))
+    ref_dir = os.path.join(HERE, "_ref")
+    lib_dir = os.path.join(ROOT, "benes_perm_b200")
+    cmd = ["g++", "-std=c++20", "-O1", "-pthread",
+           "-I", work, "-I", os.path.join(REF_DIR, "src"), "-I", os.path.join(REF_DIR, "include"),
+           "-I", os.path.join(ROOT, "include"),
+           os.path.join(work, "benes_b200_backend.cpp"), os.path.join(HERE, "shim_driver.cpp"),
+           "-L", ref_dir, "-lbenes_ref", "-L", lib_dir, "-lbenes_b200",
+           "-Wl,-rpath,$ORIGIN/..:$ORIGIN/../../../benes_perm_b200", "-o", SHIM_DRIVER + ".tmp"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError("shim build failed:\n" + proc.stderr[-4000:])
+    os.replace(SHIM_DRIVER + ".tmp", SHIM_DRIVER)
+    return SHIM_DRIVER
 
 
 class _Checker:
@@ -91,6 +143,8 @@ class Oracle(_Checker):
         L.oracle_middle_bit.argtypes = [ctypes.c_uint64, fp, ctypes.c_int, ctypes.c_void_p, u64p]
         L.oracle_factoradic_bits.argtypes = [ctypes.c_uint32]
         L.oracle_factoradic_bits.restype = ctypes.c_uint32
+        L.oracle_fill_permutation.argtypes = [ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64,
+                                              ctypes.c_uint32, ctypes.c_void_p]
 
         class _Layout(ctypes.Structure):
             _fields_ = [(n, ctypes.c_uint64) for n in (
@@ -159,6 +213,21 @@ class Oracle(_Checker):
 
     def factoradic_bits(self, c: int) -> int:
         return int(self.lib.oracle_factoradic_bits(c))
+
+    def fill_permutation(self, kind: int, seed: int, n: int, dtype=np.uint32,
+                         out: Optional[np.ndarray] = None) -> np.ndarray:
+        """The configs' seeded workload permutation (kind 0 Fisher-Yates,
+        1 Sattolo, 2 identity, 3 reverse, 4 bit reversal)."""
+        dtype = np.dtype(dtype)
+        if out is None:
+            out = np.empty(n, dtype=dtype)
+        if out.dtype != dtype or out.size != n or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous array of n values of dtype")
+        rc = self.lib.oracle_fill_permutation(int(kind), seed & (2**64 - 1), n, dtype.itemsize,
+                                              out.ctypes.data)
+        if rc:
+            raise CheckerError(rc, "invalid workload arguments")
+        return out
 
 
 class Reference(_Checker):

@@ -30,9 +30,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import Reference, make_format  # noqa: E402
+from oracle.oracle import REF_DIR, Oracle, Reference, make_format  # noqa: E402
 
-REFERENCE_GOLDEN_DIR = "/root/reference/tests/golden"
+# the reference's golden blobs (BENES_REFERENCE_DIR names its checkout)
+REFERENCE_GOLDEN_DIR = os.path.join(REF_DIR, "tests", "golden")
 
 
 def routing_depth(n: int, m: int) -> int:
@@ -44,8 +45,9 @@ def routing_depth(n: int, m: int) -> int:
 
 
 def seeded_permutation(kind: int, seed: int, n: int) -> np.ndarray:
-    import benes_perm_b200 as bp
-    return bp.fill_permutation(bp.PermutationKind(kind), seed, n, np.uint32)
+    # the oracle's restatement of the workload generator (pinned against the
+    # library's by tests/test_oracle.py)
+    return Oracle().fill_permutation(kind, seed, n, np.uint32)
 
 
 def format_cases(n: int):

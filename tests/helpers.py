@@ -40,3 +40,9 @@ def load_corpus():
 
 def corpus_permutation(bp, entry, dtype=np.uint32):
     return bp.fill_permutation(bp.PermutationKind(entry["kind"]), entry["seed"], entry["n"], dtype)
+
+
+def load_digests():
+    """SHA-256 digests of blobs the reference encoded (make_digests.py)."""
+    with open(os.path.join(GOLDEN, "reference_digests.json")) as f:
+        return json.load(f)

@@ -2,14 +2,17 @@
 """Batched and serving forms: every blob must be byte-identical to the plain
 per-request call on the same input, whether the request ran alone or mixed
 with others (sizes, widths and formats drawn like the mixed-stream
-configuration, scaled down)."""
+configuration, scaled down), and the replayed 240-request stream must give
+the reference's own bytes (digests made by tests/golden/make_digests.py with
+the reference's portable encoder)."""
 import concurrent.futures as cf
 import hashlib
 
 import numpy as np
 import pytest
 
-from helpers import b200_format, oracle_format
+import bench
+from helpers import b200_format, load_digests, oracle_format
 
 pytestmark = pytest.mark.gpu
 
@@ -132,3 +135,52 @@ def test_shrinking_then_growing_sizes(gpu, oracle):
             assert gpu.compress(perm.astype(np.uint64)) == oracle.compress(perm.astype(np.uint64))
         else:
             assert gpu.compress(perm.astype(np.uint32)) == gpu.compress(perm.astype(np.uint64))
+
+
+def _stream240(gpu):
+    d = load_digests()["stream240"]
+    specs = bench.serving_specs(d["requests"], d["max_log2"], d["seed"])
+    assert len(specs) == len(d["sha256_128"]) >= 200
+    reqs = []
+    for i, (n, kind, dtype, m, placement) in enumerate(specs):
+        perm = gpu.fill_permutation(gpu.PermutationKind(kind), d["seed"] + i, n, dtype)
+        fmt = gpu.FormatOptions(middle_group_log2=m, middle_placement=gpu.MiddlePlacement(placement))
+        reqs.append((perm, fmt))
+    return reqs, d["sha256_128"]
+
+
+def _digest(blob):
+    return hashlib.sha256(blob).hexdigest()[:32]
+
+
+def test_stream240_plain_batch_and_server_match_reference(gpu):
+    """The 240-request mixed stream (sizes up to 2^21, uint32 and uint64,
+    m in {4, 5}, every placement, Fisher-Yates and Sattolo) through the plain
+    host call, the batched device call and the serving loop: every blob
+    equals the reference's."""
+    torch = pytest.importorskip("torch")
+    reqs, want = _stream240(gpu)
+    kinds = {(p.dtype.itemsize, f.middle_group_log2, int(f.middle_placement)) for p, f in reqs}
+    assert len(kinds) == 12  # both widths x both m x three placements
+    assert max(p.size for p, _ in reqs) > (1 << 20)
+    for (perm, fmt), w in zip(reqs, want):
+        assert _digest(gpu.compress(perm, gpu.CompressOptions(format=fmt))) == w
+    items, keep = [], []
+    for perm, fmt in reqs:
+        n, width = perm.size, perm.dtype.itemsize
+        size = gpu.encoded_size(n, fmt)
+        d_in = torch.from_numpy(perm.view(np.int64 if width == 8 else np.int32)).cuda()
+        d_blob = torch.full(((size + 3) // 4 * 4,), 0xA5, dtype=torch.uint8, device="cuda")
+        keep.append((d_in, d_blob, size))
+        items.append((d_in.data_ptr(), n, width, fmt, d_blob.data_ptr(), size))
+    statuses, _ = gpu.compress_batch_device(items)
+    assert all(s == 0 for s in statuses)
+    torch.cuda.synchronize()
+    for (_, d_blob, size), w in zip(keep, want):
+        assert _digest(d_blob[:size].cpu().numpy().tobytes()) == w
+    del keep, items
+    with gpu.Server(hbm_budget_bytes=8 * 10**9, max_batch=64, workers=4) as server:
+        tickets = [server.submit(p, gpu.CompressOptions(format=f)) for p, f in reqs]
+        for t, w in zip(tickets, want):
+            blob, latency = server.wait(t)
+            assert _digest(blob) == w and latency > 0

@@ -112,3 +112,22 @@ def test_oracle_matches_reference_library(oracle, reference, b200):
                               output_clusters=comp[::-1])
                     f = oracle_format(kw)
                     assert oracle.compress(perm, f) == reference.compress(perm, f, threads=4)
+
+
+def test_workload_generator_matches_library(oracle, b200):
+    # the oracle's restatement of the seeded generator (used by the CPU
+    # baseline and the digest fixtures) gives the library's permutations
+    for kind in range(5):
+        for n in (1, 2, 3, 5, 64, 1000, 4096, 100003, 1 << 18):
+            if kind == 4 and n & (n - 1):
+                continue
+            for dt in (np.uint32, np.uint64):
+                a = oracle.fill_permutation(kind, 0x5EED + 31 * n + kind, n, dt)
+                b = b200.fill_permutation(b200.PermutationKind(kind), 0x5EED + 31 * n + kind, n, dt)
+                assert a.dtype == b.dtype and a.tobytes() == b.tobytes(), (kind, n, dt)
+    single = oracle.fill_permutation(1, 9, 4099, np.uint64)
+    seen, v = set(), 0
+    for _ in range(4099):  # Sattolo: one cycle through every value
+        seen.add(v)
+        v = int(single[v])
+    assert len(seen) == 4099 and v == 0

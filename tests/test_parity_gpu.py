@@ -13,7 +13,7 @@ import itertools
 import numpy as np
 import pytest
 
-from helpers import (b200_format, corpus_permutation, load_corpus, load_goldens,
+from helpers import (b200_format, corpus_permutation, load_corpus, load_digests, load_goldens,
                      oracle_format, routing_depth)
 
 pytestmark = pytest.mark.gpu
@@ -109,17 +109,40 @@ def test_global_levels_both_colourings(gpu, oracle, union_find_only):
 
 
 def test_partitioned_inverse_levels(gpu, oracle):
-    # nodes above 2^22 entries take the partitioned inverse and union-find
-    n = (1 << 22) + 4097
-    for kind, dtype in ((0, np.uint32), (1, np.uint64)):
-        perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0xB1C + kind, n, dtype)
-        kw = dict(middle_group_log2=4, middle_placement=2)
-        got = gpu.compress(perm, gpu.CompressOptions(format=b200_format(gpu, kw)))
-        assert got == oracle.compress(perm, oracle_format(kw)), kind
-    bad = gpu.fill_permutation(gpu.PermutationKind.uniform, 5, n)
-    bad[n // 3] = bad[n // 2]
-    with pytest.raises(ValueError):
-        gpu.compress(bad)
+    # Nodes above 2^23 entries (the walk limit) take the partitioned inverse
+    # (level_bucket + level_place, profile kind "place") and union-find
+    # colouring (no "walk" launch on that level); smaller global nodes take
+    # the plain inverse and the orbit walks.  n = 2^23 + 4097 puts level 0
+    # above the limit and level 1 below it.
+    n = (1 << 23) + 4097
+    kw = dict(middle_group_log2=4, middle_placement=2)
+    opts = gpu.CompressOptions(format=b200_format(gpu, kw))
+    gpu.set_profiling(True)
+    try:
+        for kind, dtype in ((0, np.uint32), (1, np.uint64), (0, np.uint64), (1, np.uint32)):
+            perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0xB1C + kind, n, dtype)
+            got = gpu.compress(perm, opts)
+            launches = gpu.last_profile_launches()
+            place = {lvl for k, lvl, _ in launches if k == "place"}
+            walk = {lvl for k, lvl, _ in launches if k == "walk"}
+            plain = {lvl for k, lvl, _ in launches if k == "inverse"}
+            assert place == {0} and 0 not in walk and 0 not in plain, (kind, launches[:8])
+            assert 1 in walk and 1 in plain and 1 not in place
+            assert got == oracle.compress(perm, oracle_format(kw)), (kind, dtype)
+    finally:
+        gpu.set_profiling(False)
+    # a repeated value at that size overfills one destination window of
+    # level_bucket or leaves an inverse slot unwritten: invalid_argument
+    for dtype in (np.uint32, np.uint64):
+        bad = gpu.fill_permutation(gpu.PermutationKind.uniform, 5, n, dtype)
+        bad[n // 3] = bad[n // 2]
+        with pytest.raises(ValueError, match="every value"):
+            gpu.compress(bad)
+        clash = np.zeros(n, dtype=dtype)  # n > 2^23 records for window 0: it overfills
+        with pytest.raises(ValueError, match="every value"):
+            gpu.compress(clash)
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 6, n)
+    assert gpu.compress(perm, opts) == oracle.compress(perm, oracle_format(kw))
 
 
 def test_invalid_inputs_then_recovery(gpu, oracle):
@@ -204,15 +227,19 @@ def test_config_2_one_mebi(gpu, oracle):
 
 
 @pytest.mark.slow
-def test_config_4_sattolo_100m(gpu, reference):
-    n = 100_000_007
-    perm = gpu.fill_permutation(gpu.PermutationKind.single_cycle, 4, n, np.uint64)
+def test_config_4_sattolo_100m(gpu):
+    # bytes pinned to the reference's own blob (its SHA-256, made by
+    # tests/golden/make_digests.py with the reference's portable encoder)
+    d = load_digests()["config4"]
+    n = d["n"]
+    assert n == 100_000_007
+    perm = gpu.fill_permutation(gpu.PermutationKind.single_cycle, d["seed"], n, np.uint64)
     kw = dict(middle_group_log2=4, input_clusters=[12, 11], output_clusters=[11, 12],
               middle_placement=0)
+    assert d["format"] == kw
     blob = gpu.compress(perm, gpu.CompressOptions(format=b200_format(gpu, kw)))
-    assert len(blob) == 317326221
-    want = reference.compress(perm, oracle_format(kw), threads=reference.hardware_threads())
-    assert blob == want
+    assert len(blob) == d["size"] == 317326221
+    assert hashlib.sha256(blob).hexdigest() == d["sha256"]
 
 
 def _device_round_trip(gpu, blob, perm, fmt):
@@ -273,12 +300,20 @@ def test_lookup_verifier_agrees_with_oracle_and_errors(gpu, oracle):
 
 
 @pytest.mark.slow
-def test_config_3_uniform_2p30_lookups(gpu, oracle):
-    n = 1 << 30
-    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 3, n, np.uint64)
+def test_config_3_uniform_2p30(gpu, oracle):
+    # the headline workload: 2^30 uint64 entries, m = 5, default clusters,
+    # embedded_output.  The blob must be the reference's canonical bytes (its
+    # SHA-256 from the reference's portable encoder, tests/golden/
+    # make_digests.py); a decodable blob with another valid colouring would
+    # pass lookups but not this.
+    d = load_digests()["config3"]
+    n = d["n"]
+    assert n == 1 << 30 and d["format"] == dict(middle_group_log2=5, middle_placement=2)
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, d["seed"], n, np.uint64)
     fmt = gpu.FormatOptions(5, [], [], gpu.MiddlePlacement.embedded_output)
     blob = gpu.compress(perm, gpu.CompressOptions(format=fmt))
-    assert len(blob) == 3850371096
+    assert len(blob) == d["size"] == 3850371096
+    assert hashlib.sha256(blob).hexdigest() == d["sha256"]
     _spot_check(oracle, blob, perm, count=256, seed=3)
     # every entry, both directions, on the device
     _device_round_trip(gpu, blob, perm, fmt)

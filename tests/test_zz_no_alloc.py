@@ -1,13 +1,15 @@
 # SPDX-License-Identifier: Apache-2.0
 """The allocation-free entry point, bpb200_compress_device_noalloc.
 
-It exists for callers that cannot call cudaMalloc (work captured into a CUDA
-graph, memory owned by a pooling allocator, latency-critical paths): its
-scratch is a fixed device array inside the library.  This test calls it
-through the C ABI and checks that two calls in a row produce exactly the
-bytes of the allocating entry point, bpb200_compress_device (the bar is
-byte equality: the encoding is integer work), and that sizes above its
-2^18-entry limit are rejected.  The file sorts last so a failing run that
+It exists for callers that cannot call cudaMalloc (device memory owned by a
+pooling allocator, latency-critical paths that cannot pay for an
+allocation's synchronisation): its scratch is a fixed device array inside
+the library.  This test calls it through the C ABI and checks that two
+calls in a row produce exactly the bytes of the allocating entry point,
+bpb200_compress_device (the bar is byte equality: the encoding is integer
+work), that a non-permutation is still rejected when the shared scratch
+holds an earlier call's data, and that sizes above its 2^18-entry limit are
+rejected.  The file sorts last so a failing run that
 stops at the first failure has already run every other test.
 """
 import ctypes
@@ -60,6 +62,36 @@ def test_noalloc_matches_allocating_entry_point(gpu, n, kind, dtype, fmt_kw):
         assert rc == 0, err.value.decode()
         torch.cuda.synchronize()
         assert out[:size].cpu().numpy().tobytes() == want
+
+
+def test_noalloc_rejects_duplicate_after_valid_call(gpu):
+    # the scratch keeps the previous call's inverse and status word: the
+    # per-call reset of both must still catch a repeated value
+    torch = pytest.importorskip("torch")
+    fn = _entry(gpu.library())
+    stream = torch.cuda.current_stream().cuda_stream
+    err = ctypes.create_string_buffer(256)
+    for n, dtype in ((100_003, np.uint32), (MAX_ENTRIES, np.uint64), (4_000, np.uint32)):
+        fmt = gpu.FormatOptions()
+        cfmt = gpu.to_c_format(fmt)
+        size = gpu.encoded_size(n, fmt)
+        width = np.dtype(dtype).itemsize
+        view = np.int64 if width == 8 else np.int32
+        good = gpu.fill_permutation(gpu.PermutationKind.uniform, 0xD0B + n, n, dtype)
+        bad = good.copy()
+        bad[n // 3] = bad[n // 2]
+        want = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
+        d_good = torch.from_numpy(good.view(view)).cuda()
+        gpu.compress_device(d_good.data_ptr(), n, width, want.data_ptr(), size, fmt, stream)
+        out = torch.empty_like(want)
+        for d_in, rc_want in ((d_good, 0), (torch.from_numpy(bad.view(view)).cuda(), 1),
+                              (d_good, 0)):
+            rc = fn(d_in.data_ptr(), n, width, ctypes.byref(cfmt), out.data_ptr(), size, stream,
+                    err, 256)
+            assert rc == rc_want, (n, err.value.decode())  # 1 = BPB200_INVALID_ARGUMENT
+            if rc == 0:
+                torch.cuda.synchronize()
+                assert torch.equal(out[:size], want[:size])
 
 
 def test_noalloc_rejects_oversized_input(gpu):

@@ -41,7 +41,6 @@ METRIC = "entries/sec compressed bit-exact at N=2^30; serving p50/p99 latency vs
 UNIT = "entries/s"
 SEED = 0x5EED_2030
 STREAM_TEST_SEED = 0x5EED_0240   # the mixed stream the GPU tests replay
-CPU_SAMPLE_N = 1 << 23
 
 
 def serving_specs(requests, max_log2, seed):
@@ -70,6 +69,10 @@ def parse_args():
     ap.add_argument("--log2n", type=int, default=30, help="workload size (default 30)")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-log2n", type=int, default=24,
+                    help="size of the CPU sample the reference arm and cpu_baseline time")
+    ap.add_argument("--cpu-full", action="store_true",
+                    help="reference arm: also time one full 2^30 compress (minutes)")
     ap.add_argument("--workload", default="headline", choices=("headline", "serving"),
                     help="serving: the mixed-size request stream (not the headline metric)")
     ap.add_argument("--requests", type=int, default=1024, help="serving: number of requests")
@@ -179,16 +182,22 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- roofline
 
-def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, walk_levels):
+def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, walk_levels,
+                      place_levels=()):
     """Compulsory HBM bytes per kernel kind for one compress: every array a
     kernel must touch, read once and written once at its minimal width.
     Levels in `walk_levels` are coloured by orbit walks (walk + jump), the
-    other global levels by union-find (union)."""
-    kinds = ("inverse", "union", "walk", "jump", "resolve", "output_bits", "emit", "tile")
+    other global levels by union-find (union).  Only level 0 builds an
+    inverse from its values (partitioned, kind "place", on the levels in
+    `place_levels`; else "inverse"); every later level's inverse is written
+    by its parent's output pass ("output_bits")."""
+    kinds = ("inverse", "place", "union", "walk", "jump", "resolve", "output_bits", "emit",
+             "tile")
     per = {k: 0.0 for k in kinds}
     for lvl in range(tile):
         w = entry_bytes if lvl == 0 else 4
-        per["inverse"] += (w + 4) * n              # read values, write inverse
+        if lvl == 0:
+            per["place" if lvl in place_levels else "inverse"] += (w + 4) * n
         if lvl in walk_levels:
             per["walk"] += 12 * n                  # values, inverse, owner stamp per vertex
             per["jump"] += 2 * n                   # ruler states (16 B per 16 slots) read+written
@@ -196,7 +205,8 @@ def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, wal
         else:
             per["union"] += 8 * n                  # inverse, one word per pair read+written
             per["resolve"] += (2 + w + 4) * n + n / 8  # union-find words, values, children, bits
-        per["output_bits"] += 2 * n + n / 8        # even inverse entries, bits
+        # this level's inverse, the children's inverse (when they are global), output bits
+        per["output_bits"] += 4 * n + (4 * n if lvl + 1 < tile else 0) + n / 8
         per["emit"] += n / 4                       # bits of both sides, read and placed
     w = entry_bytes if tile == 0 else 4
     per["tile"] = w * n + 2 * (depth - tile) * n / 16 + middle_bits / 8
@@ -238,18 +248,39 @@ def load_peaks():
 
 # ----------------------------------------------------------------- arms
 
-def reference_arm(args, world, rank):
-    """portable_cpu of the reference on the host cores, bounded sample."""
-    if rank != 0:
-        return
-    from oracle.oracle import Reference, make_format
-    import benes_perm_b200 as bp
+def cpu_sample_config(n_sample):
+    """Config of the CPU sample: the headline workload's format and generator
+    at a bounded size."""
+    lg = n_sample.bit_length() - 1
+    return {
+        "workload": f"compress uniform random permutation, N=2^{lg} uint64, m=5, default "
+                    "clusters, embedded_output (bounded sample of the N=2^30 workload)",
+        "n": n_sample, "entry_bytes": 8, "middle_group_log2": 5, "clusters": "balanced default",
+        "middle_placement": "embedded_output", "sample_of_n": 1 << 30,
+        "permutation": "Fisher-Yates, xoshiro256** seeded by splitmix64(0x5EED2030)",
+    }
+
+
+def _cpu_setup(n_sample):
+    """The reference library (oracle/_ref, built from the reference's own
+    sources) and the sample input, made by the oracle's restatement of the
+    workload generator: nothing of the B200 library is loaded."""
+    from oracle.oracle import Oracle, Reference, make_format
     ref = Reference()
-    threads = ref.hardware_threads()
-    n_sample = CPU_SAMPLE_N
-    perm = bp.fill_permutation(bp.PermutationKind.uniform, SEED, n_sample, np.uint64)
+    perm = Oracle().fill_permutation(0, SEED, n_sample, np.uint64)
     fmt = make_format(5, [], [], 2)
     out = np.zeros(ref.encoded_size(n_sample, fmt), dtype=np.uint8)
+    return ref, ref.hardware_threads(), perm, fmt, out
+
+
+def reference_arm(args, world, rank):
+    """portable_cpu of the reference on the host cores: each step compresses
+    a bounded sample (2^24 entries by default) of the headline workload with
+    every host thread; ``config`` names the sample actually timed."""
+    if rank != 0:
+        return
+    n_sample = 1 << args.cpu_log2n
+    ref, threads, perm, fmt, out = _cpu_setup(n_sample)
     for _ in range(args.warmup):
         ref.compress(perm, fmt, threads=threads, out=out)
     t0 = time.perf_counter()
@@ -257,30 +288,27 @@ def reference_arm(args, world, rank):
         ref.compress(perm, fmt, threads=threads, out=out)
     secs = time.perf_counter() - t0
     value = n_sample * args.steps / secs
-    n, _ = workload(args.log2n)
+    sample = (f"each step compresses a {n_sample}-entry (2^{args.cpu_log2n}) uint64 uniform "
+              f"permutation with the headline format, reference portable_cpu, {threads} threads; "
+              "a full 2^30 compress per step would not fit the run's time")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "uint64", "data": "synthetic",
-        "config": workload_config(n, args.log2n, world),
+        "config": cpu_sample_config(n_sample),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"each step compresses a {n_sample}-entry (2^23) uint64 "
-                                   "uniform permutation, same format family, portable_cpu with "
-                                   f"{threads} threads"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.cpu_full:
+        line["full_2p30"] = cpu_full_run()
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(world):
-    from oracle.oracle import Reference, make_format
-    import benes_perm_b200 as bp
-    ref = Reference()
-    threads = ref.hardware_threads()
-    perm = bp.fill_permutation(bp.PermutationKind.uniform, SEED, CPU_SAMPLE_N, np.uint64)
-    fmt = make_format(5, [], [], 2)
-    out = np.zeros(ref.encoded_size(CPU_SAMPLE_N, fmt), dtype=np.uint8)
+def cpu_baseline(args):
+    n_sample = 1 << args.cpu_log2n
+    ref, threads, perm, fmt, out = _cpu_setup(n_sample)
     ref.compress(perm, fmt, threads=threads, out=out)
     times = []
     for _ in range(3):
@@ -288,9 +316,38 @@ def cpu_baseline(world):
         ref.compress(perm, fmt, threads=threads, out=out)
         times.append(time.perf_counter() - t0)
     med = statistics.median(times)
-    return {"value": CPU_SAMPLE_N / med, "unit": UNIT, "cores": threads, "kind": "reference",
-            "sample": f"median of 3 compresses of a 2^23-entry uint64 uniform permutation (same "
-                      f"format family) by the reference portable_cpu encoder, {threads} threads"}
+    return {"value": n_sample / med, "unit": UNIT, "cores": threads, "kind": "reference",
+            "config": cpu_sample_config(n_sample),
+            "sample": f"median of 3 compresses of a 2^{args.cpu_log2n}-entry uint64 uniform "
+                      "permutation with the headline format by the reference portable_cpu "
+                      f"encoder, {threads} threads"}
+
+
+def cpu_full_run():
+    """One reference portable_cpu compress of the full 2^30 workload with all
+    host threads (minutes; about 50 GB of host memory), its bytes checked
+    against the committed reference digest."""
+    import hashlib
+    n = 1 << 30
+    ref, threads, perm, fmt, out = _cpu_setup(n)
+    t0 = time.perf_counter()
+    blob = ref.compress(perm, fmt, threads=threads, out=out)
+    secs = time.perf_counter() - t0
+    want = reference_digest(n, SEED)
+    return {"value": n / secs, "unit": UNIT, "seconds": secs, "cores": threads,
+            "kind": "reference", "n": n,
+            "sha256_matches_digest": (hashlib.sha256(blob).hexdigest() == want) if want else None}
+
+
+def reference_digest(n, seed):
+    """The committed SHA-256 of the reference's blob for the headline
+    workload at (n, seed), if tests/golden/reference_digests.json has it."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "reference_digests.json")) as f:
+            d = json.load(f)["config3"]
+    except (OSError, KeyError, ValueError):
+        return None
+    return d["sha256"] if d["n"] == n and d["seed"] == seed else None
 
 
 def b200_arm(args, world, rank, local):
@@ -338,6 +395,7 @@ def b200_arm(args, world, rank, local):
     kernel_secs = {}
     kernel_counts = {}
     walk_levels = set()
+    place_levels = set()
     with ClockSampler(gpu_index) as clocks:
         start.record(stream)
         for _ in range(args.steps):
@@ -346,7 +404,9 @@ def b200_arm(args, world, rank, local):
             for k in ks:
                 kernel_secs[k] = kernel_secs.get(k, 0.0) + ks[k] / args.steps
                 kernel_counts[k] = kc[k]
-            walk_levels |= {lvl for kind, lvl, _ in bp.last_profile_launches() if kind == "walk"}
+            marks = bp.last_profile_launches()
+            walk_levels |= {lvl for kind, lvl, _ in marks if kind == "walk"}
+            place_levels |= {lvl for kind, lvl, _ in marks if kind == "place"}
         stop.record(stream)
         torch.cuda.synchronize()
     bp.set_profiling(False)
@@ -373,7 +433,8 @@ def b200_arm(args, world, rank, local):
     e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, f"cuda:{local}")
     e2e_value = replica_throughput(n, args.e2e_steps, world, e2e_secs)
 
-    verified = verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream)
+    verified = verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream,
+                             reference_digest(n, replica_seed(rank)))
     if not verified["ok"]:
         print(f"rank {rank}: the measured blob failed verification: {verified}",
               file=sys.stderr, flush=True)
@@ -388,7 +449,7 @@ def b200_arm(args, world, rank, local):
     # its launches in a step, divided by their summed event-timed durations
     switch_bits, middle_bits = _section_bits(n, fmt)
     alg, pipeline_bytes = algorithmic_bytes(n, depth, tile, 8, switch_bits, middle_bits,
-                                            walk_levels)
+                                            walk_levels, place_levels)
     timed = {k: v for k, v in kernel_secs.items() if alg.get(k, 0) > 0 and v > 0}
     dominant = max(timed, key=timed.get)
     peak, peak_kind = load_peaks()
@@ -433,7 +494,7 @@ def b200_arm(args, world, rank, local):
         "verified": verified,
     }
     if world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(world)
+        line["cpu_baseline"] = cpu_baseline(args)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -441,12 +502,19 @@ def b200_arm(args, world, rank, local):
         sys.exit(1)
 
 
-def verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream):
-    """Checks the measured output after the timed regions: every entry of the
-    device blob round-trips through the device lookup verifier (p[i] for all
-    i, then p^-1[p[i]] == i), and the host entry point's blob equals the
+def verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream, digest):
+    """Checks the measured output after the timed regions: the blob's SHA-256
+    equals the reference's own blob's (committed digest of the reference's
+    portable encoder on this exact input, when there is one: the canonical
+    bytes, not only a decodable blob), every entry of the device blob
+    round-trips through the device lookup verifier (p[i] for all i, then
+    p^-1[p[i]] == i), and the host entry point's blob equals the
     device-resident one byte for byte."""
+    import hashlib
     t0 = time.perf_counter()
+    match = None
+    if digest is not None:
+        match = hashlib.sha256(host_blob.numpy()).hexdigest() == digest
     out = torch.empty(n, dtype=torch.int64, device=d_in.device)
     bp.lookup_device(d_blob.data_ptr(), size, n, fmt, out.data_ptr(), n,
                      stream=stream.cuda_stream)
@@ -456,9 +524,12 @@ def verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream):
     inverse = bool(torch.equal(out, torch.arange(n, dtype=torch.int64, device=d_in.device)))
     del out
     same = bool(torch.equal(host_blob.to(d_blob.device), d_blob[:size]))
-    return {"ok": forward and inverse and same, "forward_lookups": forward,
+    return {"ok": forward and inverse and same and match is not False,
+            "reference_sha256_match": match, "forward_lookups": forward,
             "inverse_lookups": inverse, "host_blob_equals_device_blob": same,
-            "method": "every entry through bpb200_lookup_device, both directions",
+            "method": "SHA-256 against the reference's blob (tests/golden/"
+                      "reference_digests.json); every entry through bpb200_lookup_device, "
+                      "both directions",
             "seconds": round(time.perf_counter() - t0, 3)}
 
 

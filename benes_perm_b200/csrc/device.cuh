@@ -170,6 +170,19 @@ __device__ __forceinline__ void uf_find_many(Word* uf, const uint32_t (&x)[K], F
 
 // K unions x(a[i]) ^ x(b[i]) == rel[i], with all 2K finds of a round in
 // lockstep.  A failed link retries from the two roots it saw.
+//
+// The first round's finds use L1-cached loads.  Once a component is large,
+// most finds end at its root, and uncached they all queue at the one L2
+// slice holding that word.  A cached word may be stale, but it still names
+// a true ancestor with its true parity, so a find ends at a node X of the
+// right component with the right relative colour; X may have stopped being
+// a root.  That is harmless: when both finds reach the same X the two nodes
+// share a component; otherwise the link is a CAS that requires the larger
+// end `hi` to be a root at that moment (it fails on a stale root, and the
+// retry rounds then read L2), and hanging a true root hi under any smaller
+// node `lo` joins two different components (a root is its component's
+// minimum, so lo < hi lies outside hi's component) while keeping parents
+// strictly decreasing.
 template <int K, typename Word>
 __device__ __forceinline__ void uf_union_many(Word* uf, uint32_t (&a)[K], uint32_t (&b)[K],
     uint32_t (&rel)[K], uint32_t pending, uint32_t* err) {
@@ -190,7 +203,7 @@ __device__ __forceinline__ void uf_union_many(Word* uf, uint32_t (&a)[K], uint32
         for (int i = 0; i < K; ++i) {
             if (pending & (1u << i)) both |= (1u << i) | (1u << (K + i));
         }
-        uf_find_many<2 * K>(uf, x, f, both, err);
+        uf_find_many<2 * K>(uf, x, f, both, err, it == 0);
 #pragma unroll
         for (int i = 0; i < K; ++i) {
             if (!(pending & (1u << i))) continue;

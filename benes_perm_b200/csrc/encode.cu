@@ -73,6 +73,7 @@ struct Workspace {
     uint32_t* h_status = nullptr; // pinned
     uint32_t* vals[2] = {nullptr, nullptr};
     uint32_t* inv = nullptr;
+    uint32_t* inv2 = nullptr;     // next level's inverse (levels alternate the two)
     uint32_t* uf = nullptr;
     uint32_t* xbits = nullptr;
     uint32_t* ybits = nullptr;
@@ -92,13 +93,14 @@ struct Workspace {
     bool busy = false;
 
     void release_scratch() {
-        for (void* p : {(void*)vals[0], (void*)vals[1], (void*)inv, (void*)uf, (void*)xbits,
+        for (void* p : {(void*)vals[0], (void*)vals[1], (void*)inv, (void*)inv2, (void*)uf,
+                 (void*)xbits,
                  (void*)ybits, (void*)owner, (void*)state[0], (void*)state[1], (void*)super_of,
                  (void*)control,
                  (void*)records, (void*)cursor, (void*)addr[0], (void*)addr[1]}) {
             if (p) cudaFree(p);
         }
-        vals[0] = vals[1] = inv = uf = xbits = ybits = owner = control = cursor = nullptr;
+        vals[0] = vals[1] = inv = inv2 = uf = xbits = ybits = owner = control = cursor = nullptr;
         super_of = nullptr;
         records = nullptr;
         state[0] = state[1] = nullptr;
@@ -180,6 +182,7 @@ void ensure_scratch(Workspace& w, const Plan& p) {
     check(cudaMalloc(&w.vals[0], slots * 4), "cudaMalloc(level array)");
     check(cudaMalloc(&w.vals[1], slots * 4), "cudaMalloc(level array)");
     check(cudaMalloc(&w.inv, slots * 4), "cudaMalloc(inverse)");
+    check(cudaMalloc(&w.inv2, slots * 4), "cudaMalloc(inverse)");
     check(cudaMalloc(&w.uf, pairs * 4), "cudaMalloc(union-find)");
     check(cudaMalloc(&w.xbits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(colour bits)");
     check(cudaMalloc(&w.ybits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(output bits)");
@@ -340,11 +343,15 @@ struct Recorder {
     }
 };
 
-// One global routing level: inverse, orbit-walk colouring (union-find only
-// when the walks give up), children, then both sections' switch bits.
+// One global routing level: inverse (level 0 only; every later level's
+// inverse comes from its parent's output pass), orbit-walk colouring
+// (union-find only when the walks give up), children, then both sections'
+// switch bits and the children's inverses.  `inv` holds this level's
+// inverse; `child_inv` receives the next level's (null when the next level
+// is the tile's, which builds its own in shared memory).
 template <typename TV>
 void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint32_t l,
-    const TV* src, uint32_t* dst, uint32_t* d_blob) {
+    const TV* src, uint32_t* dst, uint32_t* d_blob, uint32_t* inv, uint32_t* child_inv) {
     const Plan* dp = w.d_plan;
     const LevelInfo& lv = p.levels[l];
     const uint64_t slots = lv.cap << l;
@@ -362,7 +369,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
     const bool walks = lv.cap <= kWalkMaxNode && g_force_union_find.load() == 0;
     control_reset<<<1, 32, 0, st>>>(ctl, walks ? 0u : 1u);
     rec.launches += 1;
-    if (lv.cap > kWalkMaxNode && w.records != nullptr) {
+    if (l == 0 && lv.cap > kWalkMaxNode && w.records != nullptr) {
         const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
         check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
         const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kBucketThreads);
@@ -370,11 +377,11 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             level_bucket<TV><<<gb, kBucketThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
                 w.d_status);
             level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
-                w.records, w.cursor, w.inv, ctl + kCtlClaimPlace);
+                w.records, w.cursor, inv, ctl + kCtlClaimPlace);
         }, 2);
-    } else {
+    } else if (l == 0) {
         rec.launch(kKindInverse, [&] {
-            level_inverse<TV><<<gs, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.uf, w.owner,
+            level_inverse<TV><<<gs, kLevelThreads, 0, st>>>(dp, l, src, inv, w.uf, w.owner,
                 ctl + kCtlClaimInverse, w.d_status);
         });
     }
@@ -391,9 +398,9 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             const int gwalk = (int)std::max<uint64_t>(1,
                 std::min<uint64_t>((uint64_t)sms * walk_blocks_per_sm(),
                     (want + kLevelThreads - 1) / kLevelThreads));
-            level_walk<TV><<<gwalk, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner,
+            level_walk<TV><<<gwalk, kLevelThreads, 0, st>>>(dp, l, src, inv, w.owner,
                 w.state[0], ctl);
-            level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, w.inv, w.owner, ctl);
+            level_walk_short<TV><<<gp, kLevelThreads, 0, st>>>(dp, l, src, inv, w.owner, ctl);
         }, 2);
         // super-rulers of one orbit lie in one node: at most
         // (cap >> (kRulerLog2 + kSuperLog2)) + 2 of them
@@ -425,11 +432,11 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         }, one_block ? 3 : 2 + 2 * (rounds + 1));
     }
     rec.launch(kKindUnion, [&] {
-        level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard,
+        level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, inv, w.uf, ctl + kCtlHard,
             ctl + kCtlClaimUnion, w.d_status);
     });
     rec.launch(kKindOrient, [&] {
-        level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, w.inv, w.uf, ctl + kCtlHard, w.d_status);
+        level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, inv, w.uf, ctl + kCtlHard, w.d_status);
     });
     rec.launch(kKindResolve, [&] {
         const uint32_t supers = (buckets + (1u << kSuperLog2) - 1) >> kSuperLog2;
@@ -437,7 +444,11 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             w.state[1], w.state[1] + supers, w.uf, w.xbits, dst, ctl, w.d_status);
     });
     rec.launch(kKindOutputBits, [&] {
-        level_ybits<<<gp, kLevelThreads, 0, st>>>(dp, l, w.inv, w.xbits, w.ybits);
+        // the next level's walk owners start unset and its pair-nodes as
+        // roots; the tile level keeps its own state in shared memory
+        const bool global_child = child_inv != nullptr;
+        level_outputs<<<gp, kLevelThreads, 0, st>>>(dp, l, inv, w.xbits, w.ybits, child_inv,
+            global_child ? w.owner : nullptr, global_child ? w.uf : nullptr);
     });
     for (int side = 0; side < 2; ++side) {
         const LevelSide& ls = lv.side[side];
@@ -516,13 +527,15 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         check(cudaMemsetAsync(w.inv, 0xff, p.levels[0].cap * 4, st), "cudaMemsetAsync");
     }
     const uint32_t* cur32 = nullptr;
+    uint32_t* invs[2] = {w.inv, w.inv2};
     for (uint32_t l = 0; l < t0; ++l) {
         rec.level = (int)l;
         uint32_t* dst = w.vals[l & 1];
+        uint32_t* child_inv = l + 1 < t0 ? invs[(l + 1) & 1] : nullptr;
         if (l == 0) {
-            run_level<T>(w, rec, st, p, l, d_in, dst, d_blob);
+            run_level<T>(w, rec, st, p, l, d_in, dst, d_blob, invs[0], child_inv);
         } else {
-            run_level<uint32_t>(w, rec, st, p, l, cur32, dst, d_blob);
+            run_level<uint32_t>(w, rec, st, p, l, cur32, dst, d_blob, invs[l & 1], child_inv);
         }
         cur32 = dst;
     }
@@ -1001,7 +1014,8 @@ constexpr size_t kOffStatus = kOffPlan + up256(sizeof(Plan));
 constexpr size_t kOffVals0 = kOffStatus + 256;
 constexpr size_t kOffVals1 = kOffVals0 + up256(kSlots * 4);
 constexpr size_t kOffInv = kOffVals1 + up256(kSlots * 4);
-constexpr size_t kOffUf = kOffInv + up256(kSlots * 4);
+constexpr size_t kOffInv2 = kOffInv + up256(kSlots * 4);
+constexpr size_t kOffUf = kOffInv2 + up256(kSlots * 4);
 constexpr size_t kOffXbits = kOffUf + up256(kPairs * 4);
 constexpr size_t kOffYbits = kOffXbits + up256((kPairs / 32 + 1) * 4);
 constexpr size_t kOffAddr0 = kOffYbits + up256((kPairs / 32 + 1) * 4);
@@ -1011,7 +1025,8 @@ constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
 constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffSuper = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffControl = kOffSuper + up256(((kSlots >> kRulerLog2) + 1) * 4);
-constexpr size_t kBytes = kOffControl + 256; // under 7 MB
+constexpr size_t kBytes = kOffControl + 256; // under 8 MB
+static_assert(kBytes < (8u << 20), "allocation-free scratch stays under 8 MB");
 
 } // namespace noalloc
 } // namespace bpb200
@@ -1088,6 +1103,7 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         w.vals[0] = reinterpret_cast<uint32_t*>(base + noalloc::kOffVals0);
         w.vals[1] = reinterpret_cast<uint32_t*>(base + noalloc::kOffVals1);
         w.inv = reinterpret_cast<uint32_t*>(base + noalloc::kOffInv);
+        w.inv2 = reinterpret_cast<uint32_t*>(base + noalloc::kOffInv2);
         w.uf = reinterpret_cast<uint32_t*>(base + noalloc::kOffUf);
         w.xbits = reinterpret_cast<uint32_t*>(base + noalloc::kOffXbits);
         w.ybits = reinterpret_cast<uint32_t*>(base + noalloc::kOffYbits);

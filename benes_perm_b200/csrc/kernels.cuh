@@ -18,7 +18,8 @@
 //                colour 0), or the orbit-walk colour on walk levels;
 //                children left[k] = p[2k+x]/2, right[k] = p[2k+1-x]/2; the
 //                input switch of pair k is x(k)
-//   ybits        output switch of output pair k is colour(inv[2k])
+//   outputs      output switch of output pair k is colour(inv[2k]); the
+//                children's inverses follow from the same two reads
 //   emit         switch bits into the clustered blob layout: word copies of
 //                long packet runs, word blocks of short ones, bits for the
 //                rest
@@ -367,13 +368,34 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
     }
 }
 
-// Output switch bits in natural (node, output pair) order.
-__global__ void __launch_bounds__(256) level_ybits(const Plan* __restrict__ plan,
+// Output side of a level, in natural (node, output pair) order: the output
+// switch bits and the children's inverses, so no level below the first
+// scatters an inverse.  Output pair k of node j joins outputs 2k and 2k+1,
+// fed by inputs u0 = inv[2k] and u1 = inv[2k+1], whose colours differ.  Its
+// switch bit is y = colour(u0) (src/benes.cpp:306-310: the output bit of
+// input i is colour(i) ^ (p[i] & 1), and p[u0] = 2k).  Of the two, the
+// colour-0 input inv[2k + y] is routed to the left child, where it sits at
+// input pair inv[2k + y] >> 1 and carries value k (src/benes.cpp:313-314);
+// the other goes right with the same value.  So
+//     left_inv[k] = inv[2k + y] >> 1,  right_inv[k] = inv[2k + 1 - y] >> 1,
+// and an odd node's tail output s - 1, whose input is coloured 0, gives
+// left_inv[s / 2] = inv[s - 1] >> 1.  The pass reads inv sequentially and
+// one colour bit per output pair, and writes the children's inverse
+// sequentially.  It also resets the children's per-slot walk owners and
+// pair-node union-find roots (`child_owner` / `child_uf`, may be null), the
+// state the next level's colouring starts from.  A value out of range (only
+// possible when the input was not a permutation, which level 0 reports)
+// leaves 0xffffffff, which every user range-checks.
+__global__ void __launch_bounds__(256) level_outputs(const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, const uint32_t* __restrict__ xbits,
-    uint32_t* __restrict__ ybits) {
+    uint32_t* __restrict__ ybits, uint32_t* __restrict__ child_inv,
+    uint32_t* __restrict__ child_owner, uint32_t* __restrict__ child_uf) {
     const LevelInfo& lv = plan->levels[level];
+    const LevelInfo& cl = plan->levels[level + 1];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
+    const uint32_t ccap = (uint32_t)cl.cap;
+    const uint32_t cpcap = (uint32_t)cl.pcap;
     const uint64_t total = (uint64_t)pcap << level;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -383,11 +405,43 @@ __global__ void __launch_bounds__(256) level_ybits(const Plan* __restrict__ plan
             const uint32_t j = (uint32_t)(p / pcap);
             const uint32_t k = (uint32_t)(p - (uint64_t)j * pcap);
             const uint32_t s = size_at(lv, level, j);
-            if (k < s / 2) {
-                const uint32_t u = inv[(uint64_t)j * cap + 2 * k];
-                if (u < s) {
-                    const uint64_t q = (uint64_t)j * pcap + (u >> 1);
-                    y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+            const uint32_t half = s / 2;
+            const uint64_t node = (uint64_t)j * cap;
+            const uint64_t lb = (uint64_t)(2 * j) * ccap;
+            const uint64_t rb = lb + ccap;
+            if (k < half) {
+                const uint32_t u0 = inv[node + 2 * k];
+                const uint32_t u1 = inv[node + 2 * k + 1];
+                uint32_t to_left = ~0u, to_right = ~0u;
+                if (u0 < s && u1 < s) {
+                    const uint64_t q = (uint64_t)j * pcap + (u0 >> 1);
+                    y = (((xbits[q >> 5] >> (q & 31)) ^ u0) & 1u) != 0;
+                    to_left = (y ? u1 : u0) >> 1;
+                    to_right = (y ? u0 : u1) >> 1;
+                }
+                if (child_inv != nullptr) {
+                    child_inv[lb + k] = to_left;
+                    child_inv[rb + k] = to_right;
+                }
+                if (child_owner != nullptr) {
+                    child_owner[lb + k] = ~0u;
+                    child_owner[rb + k] = ~0u;
+                }
+            } else if (k == half && (s & 1u) != 0) {
+                const uint32_t u = inv[node + s - 1];
+                if (child_inv != nullptr) child_inv[lb + half] = u < s ? u >> 1 : ~0u;
+                if (child_owner != nullptr) child_owner[lb + half] = ~0u;
+            }
+            // children's pair-nodes start as their own roots: left child of
+            // s - s/2 entries, right of s/2; pair-node k/2 for even k
+            if (child_uf != nullptr && (k & 1u) == 0) {
+                if (k < s - half) {
+                    const uint32_t id = 2 * j * cpcap + (k >> 1);
+                    child_uf[id] = id << 1;
+                }
+                if (k < half) {
+                    const uint32_t id = (2 * j + 1) * cpcap + (k >> 1);
+                    child_uf[id] = id << 1;
                 }
             }
         }

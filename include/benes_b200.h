@@ -87,7 +87,7 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
  * can imply.  Same arguments and result bytes as bpb200_compress_device
  * (device input and blob, work queued on `stream`), but every byte of
  * scratch comes from one fixed device array inside this library (under
- * 7 MB, present on every GPU that loads the library until the process
+ * 8 MB, present on every GPU that loads the library until the process
  * exits), so it accepts at most 262144 (2^18) entries and returns
  * BPB200_LENGTH above that.  It calls no cudaMalloc/cudaFree.  Like
  * bpb200_compress_device, each call uploads its plan from host memory,

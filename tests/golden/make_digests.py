@@ -19,8 +19,10 @@ the B200 library.  Sets:
   up to 2^24).
 
 The stream specifications come from ``bench.serving_specs`` (numpy only).
-Usage: python tests/golden/make_digests.py [set ...]   (needs oracle/_ref).
-The 2^30 set needs about 50 GB of host memory and several minutes.
+Usage: python tests/golden/make_digests.py [--out FILE] [set ...]
+(needs oracle/_ref).  The 2^30 set needs about 70 GB of host memory and
+several minutes; ``--out`` writes the sets made by this run to FILE instead
+(to merge into this directory's file afterwards).
 """
 from __future__ import annotations
 
@@ -55,18 +57,18 @@ STREAMS = {
 }
 
 
-def load() -> dict:
-    if os.path.exists(OUT):
-        with open(OUT) as f:
+def load(path: str) -> dict:
+    if os.path.exists(path):
+        with open(path) as f:
             return json.load(f)
     return {}
 
 
-def save(d: dict) -> None:
-    with open(OUT + ".tmp", "w") as f:
+def save(d: dict, path: str) -> None:
+    with open(path + ".tmp", "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
         f.write("\n")
-    os.replace(OUT + ".tmp", OUT)
+    os.replace(path + ".tmp", path)
 
 
 def single(name: str, ref: Reference, oracle: Oracle, threads: int) -> dict:
@@ -95,18 +97,21 @@ def stream(name: str, ref: Reference, oracle: Oracle, threads: int) -> dict:
 
 
 def main(argv) -> None:
+    out = OUT
+    if argv[:1] == ["--out"]:
+        out, argv = argv[1], argv[2:]
     names = argv or list(SINGLE) + list(STREAMS)
     ref, oracle = Reference(), Oracle()
     threads = ref.hardware_threads()
     for name in names:
-        d = load()
+        d = load(out)
         if name in SINGLE:
             d[name] = single(name, ref, oracle, threads)
         elif name in STREAMS:
             d[name] = stream(name, ref, oracle, threads)
         else:
             raise SystemExit(f"unknown set {name}")
-        save(d)
+        save(d, out)
         print(name, "done", flush=True)
 
 

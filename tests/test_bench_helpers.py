@@ -31,3 +31,30 @@ def test_pipeline_bytes_of_the_2p30_workload(b200):
     assert abs(pipeline / 227.2e9 - 1) < 1e-3          # about 227.2 GB per compress
     # every level's kernels are charged: kinds sum to more than one pass per level
     assert sum(per.values()) > 8 * n * tile
+
+
+def test_reference_arm_loads_nothing_of_the_b200_library(tmp_path):
+    """bench.py --impl reference times the reference library alone: its
+    input comes from the oracle's generator, and neither the package nor
+    libbenes_b200.so is loaded in that process."""
+    import json
+    import os
+    import subprocess
+    import sys
+    from oracle.oracle import REF_SO
+    if not os.path.exists(REF_SO):
+        pytest.skip("oracle/_ref is not built")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import sys; sys.argv = ['bench.py', '--impl', 'reference', '--steps', '2', "
+            "'--warmup', '1', '--cpu-log2n', '14']; import bench; bench.main(); "
+            "maps = open('/proc/self/maps').read(); "
+            "print('LOADED' if ('libbenes_b200' in maps or 'benes_perm_b200' in sys.modules) "
+            "else 'CLEAN')")
+    run = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True,
+                         timeout=300)
+    assert run.returncode == 0, run.stderr[-2000:]
+    lines = run.stdout.strip().splitlines()
+    assert lines[-1] == "CLEAN"
+    line = json.loads(lines[-2])
+    assert line["impl"] == "reference" and line["config"]["n"] == 1 << 14
+    assert line["value"] > 0 and line["cpu_baseline"]["cores"] >= 1

@@ -352,11 +352,11 @@ class _Request(ctypes.Structure):
     ]
 
 
-def compress_batch_device(items, stream: int = 0):
+def compress_batch_device(items, stream: int = 0, raise_errors: bool = True):
     """Batched form: ``items`` is a list of
     (d_entries, count, entry_bytes, FormatOptions, d_blob, blob_len) with
     device pointers.  Returns (statuses, kernel launches); raises for the
-    first failing request."""
+    first failing request unless ``raise_errors`` is false."""
     lib = library()
     arr = (_Request * len(items))()
     for i, (d_in, n, width, fmt, d_blob, blob_len) in enumerate(items):
@@ -371,7 +371,7 @@ def compress_batch_device(items, stream: int = 0):
                                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32)]
     rc = lib.bpb200_compress_batch(arr, len(items), stream, ctypes.byref(launches))
     statuses = [arr[i].status for i in range(len(items))]
-    if rc != 0:
+    if rc != 0 and raise_errors:
         bad = next(i for i, s in enumerate(statuses) if s != 0)
         raise_for(statuses[bad], arr[bad].error.decode())
     return statuses, launches.value

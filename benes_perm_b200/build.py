@@ -18,7 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbenes_b200.so")
 SOURCES = ["encode.cu", "layout.cpp", "permgen.cpp"]
 HEADERS = ["plan.hpp", "layout.hpp", "device.cuh", "kernels.cuh", "tile.cuh", "walk.cuh",
-           "serve.inc", "file.inc", "staging.inc", "lookup.hpp", "lookup.inc"]
+           "batch_levels.cuh", "group.inc", "serve.inc", "file.inc", "staging.inc", "lookup.hpp",
+           "lookup.inc"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

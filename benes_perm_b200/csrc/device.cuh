@@ -11,6 +11,17 @@
 
 namespace bpb200 {
 
+// The block's place in the grid it works in: the launch's own grid for a
+// one-permutation launch, or this permutation's share of the blocks of a
+// batched launch over many permutations (serve.inc).  Kernel bodies index
+// their work by it instead of blockIdx / gridDim.
+struct Grid {
+    uint32_t bid;
+    uint32_t nblk;
+};
+
+__device__ __forceinline__ Grid launch_grid() { return Grid{blockIdx.x, gridDim.x}; }
+
 // Device status word bits (read by the host after each call).
 constexpr uint32_t kErrNotPermutation = 1u;  // value out of range or duplicated
 constexpr uint32_t kErrIterationCap = 2u;    // a bounded retry loop gave up

@@ -8,6 +8,7 @@
 // memory.  Everything runs on one stream; scratch lives in a pooled
 // per-device workspace so repeated calls allocate nothing.
 #include "../../include/benes_b200.h"
+#include "batch_levels.cuh"
 #include "kernels.cuh"
 #include "layout.hpp"
 #include "plan.hpp"
@@ -343,6 +344,39 @@ struct Recorder {
     }
 };
 
+// The emission launches of one section at one level, in launch order:
+// f(form, full, blocks) per launch.  Packet runs of at least 32 switches
+// are copied word-wise; shorter runs go out as whole words where every node
+// fills the packet (transposed across 32 nodes when a cluster root holds at
+// least 32 nodes, else gathered per word), and the tail packets bit by bit
+// (`full` is the number of full packets, the first packet of the per-bit
+// form).
+template <typename F>
+void emission_launches(const Plan& p, uint32_t l, int side, F&& f) {
+    const LevelInfo& lv = p.levels[l];
+    const LevelSide& ls = lv.side[side];
+    const uint32_t span_log2 = p.groups[side][ls.group].depth - ls.rel - 1;
+    const uint64_t packets = (lv.cap / 2 + (1ull << span_log2) - 1) >> span_log2;
+    if (span_log2 >= 5) {
+        f((int)kEmitWords, 0ull, grid_for(packets << (l + span_log2 - 5), kLevelThreads));
+        return;
+    }
+    const uint64_t half_min = lv.q / 2;
+    const uint64_t full = half_min >= 1 ? (half_min - 1) >> span_log2 : 0;
+    const uint32_t rel = ls.rel;
+    const uint32_t per_word_log2 = std::min<uint32_t>(5 - span_log2, rel);
+    if (full > 0 && rel >= 5) {
+        const uint64_t windows = (full + (32 >> span_log2) - 1) >> (5 - span_log2);
+        const uint64_t threads = (windows << (l - 5)) * 32;
+        f((int)kEmitTranspose, full, grid_for(threads, kLevelThreads));
+    } else if (full > 0) {
+        const uint64_t words = (full << (rel - per_word_log2)) << (l - rel);
+        f((int)kEmitBlocks, full, grid_for(words, kLevelThreads));
+    }
+    f((int)kEmitBits, full,
+        grid_for((packets - std::min(packets, full)) << (l + span_log2), kLevelThreads));
+}
+
 // One global routing level: inverse (level 0 only; every later level's
 // inverse comes from its parent's output pass), orbit-walk colouring
 // (union-find only when the walks give up), children, then both sections'
@@ -451,46 +485,29 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             global_child ? w.owner : nullptr, global_child ? w.uf : nullptr);
     });
     for (int side = 0; side < 2; ++side) {
-        const LevelSide& ls = lv.side[side];
-        const uint32_t span_log2 = p.groups[side][ls.group].depth - ls.rel - 1;
-        const uint64_t packets = (lv.cap / 2 + (1ull << span_log2) - 1) >> span_log2;
         const uint32_t* bits = side == 0 ? w.xbits : w.ybits;
-        if (span_log2 >= 5) {
-            // runs of at least 32 switches: copy whole words
-            const int ge = grid_for(packets << (l + span_log2 - 5), kLevelThreads);
+        emission_launches(p, l, side, [&](int form, uint64_t full, int blocks) {
             rec.launch(kKindEmit, [&] {
-                level_emit_words<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side],
-                    d_blob);
+                switch (form) {
+                case kEmitWords:
+                    level_emit_words<<<blocks, kLevelThreads, 0, st>>>(dp, l, side, bits,
+                        w.addr[side], d_blob);
+                    break;
+                case kEmitTranspose:
+                    level_emit_transpose<<<blocks, kLevelThreads, 0, st>>>(dp, l, side, bits,
+                        w.addr[side], d_blob, full);
+                    break;
+                case kEmitBlocks:
+                    level_emit_blocks<<<blocks, kLevelThreads, 0, st>>>(dp, l, side, bits,
+                        w.addr[side], d_blob, full);
+                    break;
+                default:
+                    level_emit<<<blocks, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side],
+                        d_blob, full);
+                    break;
+                }
             });
-        } else {
-            // packets below the smallest node's tail packet: whole-word
-            // blocks; the rest (tail packets) bit by bit
-            const uint64_t half_min = lv.q / 2;
-            const uint64_t full = half_min >= 1 ? (half_min - 1) >> span_log2 : 0;
-            const uint32_t rel = ls.rel;
-            const uint32_t per_word_log2 = std::min<uint32_t>(5 - span_log2, rel);
-            if (full > 0 && rel >= 5) {
-                // roots of >= 32 nodes: warps of 32 nodes transpose their bits
-                const uint64_t windows = (full + (32 >> span_log2) - 1) >> (5 - span_log2);
-                const uint64_t threads = (windows << (l - 5)) * 32;
-                rec.launch(kKindEmit, [&] {
-                    level_emit_transpose<<<grid_for(threads, kLevelThreads), kLevelThreads, 0,
-                        st>>>(dp, l, side, bits, w.addr[side], d_blob, full);
-                });
-            } else if (full > 0) {
-                const uint64_t words = (full << (rel - per_word_log2)) << (l - rel);
-                rec.launch(kKindEmit, [&] {
-                    level_emit_blocks<<<grid_for(words, kLevelThreads), kLevelThreads, 0, st>>>(
-                        dp, l, side, bits, w.addr[side], d_blob, full);
-                });
-            }
-            const int ge = grid_for((packets - std::min(packets, full)) << (l + span_log2),
-                kLevelThreads);
-            rec.launch(kKindEmit, [&] {
-                level_emit<<<ge, kLevelThreads, 0, st>>>(dp, l, side, bits, w.addr[side], d_blob,
-                    full);
-            });
-        }
+        });
     }
     check(cudaGetLastError(), "level kernel launch");
 }

@@ -74,7 +74,7 @@ __device__ __forceinline__ uint32_t size_at(const LevelInfo& lv, uint32_t level,
 // ------------------------------------------------------------ level kernels
 
 template <typename T>
-__global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_inverse_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint32_t* __restrict__ inv,
     uint32_t* __restrict__ uf, uint32_t* __restrict__ owner, uint32_t* claims, uint32_t* status) {
     const LevelInfo& lv = plan->levels[level];
@@ -142,6 +142,13 @@ __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ pl
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ src, uint32_t* __restrict__ inv,
+    uint32_t* __restrict__ uf, uint32_t* __restrict__ owner, uint32_t* claims, uint32_t* status) {
+    level_inverse_run<T>(launch_grid(), plan, level, src, inv, uf, owner, claims, status);
+}
+
 // ---------------------------------------------------------------------------
 // Partitioned inverse for levels whose nodes do not fit in L2.  A plain
 // scatter inv[p[i]] = i there costs one HBM read-modify-write of a 32-byte
@@ -172,7 +179,7 @@ constexpr int kBucketItems = 16;
 constexpr int kBucketThreads = BPB200_BUCKET_THREADS; // block size of level_bucket
 
 template <typename T>
-__global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_bucket_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
     uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
     __shared__ uint32_t count[kMaxWindows];
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan
     const uint32_t windows = (uint32_t)((total + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
     const uint64_t chunk = (uint64_t)blockDim.x * kBucketItems;
     const bool aligned = ((uintptr_t)src & 15u) == 0;
-    for (uint64_t c0 = (uint64_t)blockIdx.x * chunk; c0 < total; c0 += (uint64_t)gridDim.x * chunk) {
+    for (uint64_t c0 = (uint64_t)grid.bid * chunk; c0 < total; c0 += (uint64_t)grid.nblk * chunk) {
         for (uint32_t b = threadIdx.x; b < windows; b += blockDim.x) count[b] = 0;
         __syncthreads();
         const uint64_t e0 = c0 + (uint64_t)threadIdx.x * kBucketItems;
@@ -250,9 +257,16 @@ __global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
+    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
+    level_bucket_run<T>(launch_grid(), plan, level, src, records, cursor, uf, status);
+}
+
 constexpr int kPlaceItems = 16;
 
-__global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_place_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const uint2* __restrict__ records, const uint32_t* __restrict__ cursor,
     uint32_t* __restrict__ inv, uint32_t* claims) {
     const LevelInfo& lv = plan->levels[level];
@@ -273,11 +287,17 @@ __global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan
     }
 }
 
+__global__ void __launch_bounds__(256) level_place(const Plan* __restrict__ plan,
+    uint32_t level, const uint2* __restrict__ records, const uint32_t* __restrict__ cursor,
+    uint32_t* __restrict__ inv, uint32_t* claims) {
+    level_place_run(launch_grid(), plan, level, records, cursor, inv, claims);
+}
+
 // Blocks claim chunks of output pairs in address order (claim_chunk), so the
 // union-find words being linked at any time belong to the few nodes those
 // chunks cover: once a node's words fit in L2 the random finds hit there.
 // `hard` was written by earlier launches: all threads see the same value.
-__global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) level_union(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_union_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard,
     uint32_t* claims, uint32_t* status) {
     if (hard != nullptr && *hard == 0) {
@@ -332,7 +352,13 @@ __global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) level_union(cons
     }
 }
 
-__global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
+__global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) level_union(const Plan* __restrict__ plan,
+    uint32_t level, const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard,
+    uint32_t* claims, uint32_t* status) {
+    level_union_run(launch_grid(), plan, level, inv, uf, hard, claims, status);
+}
+
+__device__ __forceinline__ void level_orient_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard, uint32_t* status) {
     if (hard != nullptr && *hard == 0) {
         return;
@@ -341,8 +367,8 @@ __global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t nodes = 1ull << level;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nodes;
-         j += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t j = (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes;
+         j += (uint64_t)grid.nblk * blockDim.x) {
         const uint32_t s = size_at(lv, level, (uint32_t)j);
         if ((s & 1u) == 0) {
             continue;
@@ -358,14 +384,24 @@ __global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
     }
 }
 
-__global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
+__global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
+    const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard, uint32_t* status) {
+    level_orient_run(launch_grid(), plan, level, inv, uf, hard, status);
+}
+
+__device__ __forceinline__ void level_descriptors_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     NodeAddress* __restrict__ in_addr, NodeAddress* __restrict__ out_addr) {
     const uint64_t nodes = 1ull << level;
-    for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nodes;
-         j += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t j = (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes;
+         j += (uint64_t)grid.nblk * blockDim.x) {
         in_addr[j] = node_address(*plan, 0, level, j);
         out_addr[j] = node_address(*plan, 1, level, j);
     }
+}
+
+__global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
+    NodeAddress* __restrict__ in_addr, NodeAddress* __restrict__ out_addr) {
+    level_descriptors_run(launch_grid(), plan, level, in_addr, out_addr);
 }
 
 // Output side of a level, in natural (node, output pair) order: the output
@@ -386,7 +422,7 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
 // state the next level's colouring starts from.  A value out of range (only
 // possible when the input was not a permutation, which level 0 reports)
 // leaves 0xffffffff, which every user range-checks.
-__global__ void __launch_bounds__(256) level_outputs(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const uint32_t* __restrict__ inv, const uint32_t* __restrict__ xbits,
     uint32_t* __restrict__ ybits, uint32_t* __restrict__ child_inv,
     uint32_t* __restrict__ child_owner, uint32_t* __restrict__ child_uf) {
@@ -397,8 +433,8 @@ __global__ void __launch_bounds__(256) level_outputs(const Plan* __restrict__ pl
     const uint32_t ccap = (uint32_t)cl.cap;
     const uint32_t cpcap = (uint32_t)cl.pcap;
     const uint64_t total = (uint64_t)pcap << level;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
+    for (uint64_t p = (uint64_t)grid.bid * blockDim.x + threadIdx.x;
          p - (threadIdx.x & 31) < total; p += stride) {
         bool y = false;
         if (p < total) {
@@ -452,11 +488,18 @@ __global__ void __launch_bounds__(256) level_outputs(const Plan* __restrict__ pl
     }
 }
 
+__global__ void __launch_bounds__(256) level_outputs(const Plan* __restrict__ plan,
+    uint32_t level, const uint32_t* __restrict__ inv, const uint32_t* __restrict__ xbits,
+    uint32_t* __restrict__ ybits, uint32_t* __restrict__ child_inv,
+    uint32_t* __restrict__ child_owner, uint32_t* __restrict__ child_uf) {
+    level_outputs_run(launch_grid(), plan, level, inv, xbits, ybits, child_inv, child_owner, child_uf);
+}
+
 // Switch bits of one section at one level, packet-major: thread t maps to
 // (packet, node, pair-in-span) with the pair fastest, then the node, so for
 // full packets consecutive threads land on consecutive blob bits and a
 // warp issues one or two atomics instead of one per bit.
-__global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_emit_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, int side, const uint32_t* __restrict__ bits,
     const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t first_packet) {
     const LevelInfo& lv = plan->levels[level];
@@ -469,8 +512,8 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
     const uint32_t shift = level + span_log2; // log2(nodes * span)
     const uint64_t total = packets > first_packet ? (packets - first_packet) << shift : 0;
     const uint64_t section_bit = plan->section_offset[side] * 8;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
+    for (uint64_t t = (uint64_t)grid.bid * blockDim.x + threadIdx.x;
          t - (threadIdx.x & 31) < total; t += stride) {
         bool set = false;
         uint64_t dest = 0;
@@ -492,6 +535,12 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
     }
 }
 
+__global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t first_packet) {
+    level_emit_run(launch_grid(), plan, level, side, bits, addr, blob, first_packet);
+}
+
 // Block form of level_emit for short runs (span_log2 < 5), on the packets
 // every node of the level fills (packet < full_packets: below the smallest
 // node's tail packet, so every node contributes `span` switches and every
@@ -500,7 +549,7 @@ __global__ void __launch_bounds__(256) level_emit(const Plan* __restrict__ plan,
 // level's switches of one cluster root are then one contiguous block,
 // path-major: thread per 32-bit word of a block, gathering the `span`-bit
 // fields of 32 / span consecutive nodes, one or two atomics per word.
-__global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_emit_blocks_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, int side, const uint32_t* __restrict__ bits,
     const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
     const LevelInfo& lv = plan->levels[level];
@@ -516,8 +565,8 @@ __global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict_
     const uint64_t per_root = full_packets << words_log2;
     const uint64_t total = (per_root << (level - rel));
     const uint64_t section_bit = plan->section_offset[side] * 8;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
+    for (uint64_t t = (uint64_t)grid.bid * blockDim.x + threadIdx.x; t < total; t += stride) {
         const uint64_t root = t / per_root;
         const uint64_t rem = t - root * per_root;
         const uint64_t packet = rem >> words_log2;
@@ -544,6 +593,12 @@ __global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict_
     }
 }
 
+__global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
+    level_emit_blocks_run(launch_grid(), plan, level, side, bits, addr, blob, full_packets);
+}
+
 // Transposed form of level_emit_blocks for cluster roots of at least 32
 // nodes (rel >= 5): a warp takes 32 consecutive nodes of one root and a
 // window of 32 / span full packets.  Each lane loads one 32-bit window of
@@ -551,7 +606,7 @@ __global__ void __launch_bounds__(256) level_emit_blocks(const Plan* __restrict_
 // and lane L then assembles output word L with 32 / span shuffles: packet
 // L / span of the window, nodes (L % span) * 32 / span onwards.  Two loads
 // per lane replace the 2 * 32 / span loads per word of the block form.
-__global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_emit_transpose_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, int side, const uint32_t* __restrict__ bits,
     const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
     const LevelInfo& lv = plan->levels[level];
@@ -567,8 +622,8 @@ __global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restri
     const uint64_t total_warps = groups * windows;
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint32_t lane = threadIdx.x & 31;
-    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t wi = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; wi < total_warps;
+    const uint64_t warps = ((uint64_t)grid.nblk * blockDim.x) >> 5;
+    for (uint64_t wi = ((uint64_t)grid.bid * blockDim.x + threadIdx.x) >> 5; wi < total_warps;
          wi += warps) {
         const uint64_t group = wi / windows;
         const uint64_t k0 = (wi - group * windows) << per_window_log2;
@@ -605,6 +660,12 @@ __global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restri
     }
 }
 
+__global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob, uint64_t full_packets) {
+    level_emit_transpose_run(launch_grid(), plan, level, side, bits, addr, blob, full_packets);
+}
+
 // Word-wise form of level_emit for levels whose packets carry at least 32
 // switches of each node (span_log2 >= 5).  The switches of one node inside
 // one packet are a contiguous run of the node's bits and land on a
@@ -613,7 +674,7 @@ __global__ void __launch_bounds__(256) level_emit_transpose(const Plan* __restri
 // 32-switch chunk, one funnel shift to align the source and one or two
 // atomics for the destination words (neighbouring runs share edge words).
 // Chunks start at multiples of 32 pairs, so a chunk never crosses a packet.
-__global__ void __launch_bounds__(256) level_emit_words(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_emit_words_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, int side, const uint32_t* __restrict__ bits,
     const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob) {
     const LevelInfo& lv = plan->levels[level];
@@ -627,8 +688,8 @@ __global__ void __launch_bounds__(256) level_emit_words(const Plan* __restrict__
     const uint32_t shift = level + cshift;  // log2(nodes * chunks per run)
     const uint64_t total = packets << shift;
     const uint64_t section_bit = plan->section_offset[side] * 8;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += stride) {
+    const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
+    for (uint64_t t = (uint64_t)grid.bid * blockDim.x + threadIdx.x; t < total; t += stride) {
         const uint64_t packet = t >> shift;
         const uint64_t rem = t & ((1ull << shift) - 1);
         const uint32_t node = (uint32_t)(rem >> cshift);
@@ -654,6 +715,12 @@ __global__ void __launch_bounds__(256) level_emit_words(const Plan* __restrict__
             atomicOr(blob + (dest >> 5) + 1, v >> (32 - off));
         }
     }
+}
+
+__global__ void __launch_bounds__(256) level_emit_words(const Plan* __restrict__ plan,
+    uint32_t level, int side, const uint32_t* __restrict__ bits,
+    const NodeAddress* __restrict__ addr, uint32_t* __restrict__ blob) {
+    level_emit_words_run(launch_grid(), plan, level, side, bits, addr, blob);
 }
 
 } // namespace bpb200

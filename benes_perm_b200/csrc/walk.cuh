@@ -131,7 +131,7 @@ struct NodeView {
 // longest walk.  state[r] = {next ruler, min key, min mirror key, 0};
 // owner[slot] = r for every real vertex the walk passes.
 template <typename T>
-__global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan, uint32_t level,
+__device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     const T* __restrict__ vals, const uint32_t* __restrict__ inv, uint32_t* __restrict__ owner,
     uint4* __restrict__ state, uint32_t* control) {
     const LevelInfo& lv = plan->levels[level];
@@ -215,6 +215,13 @@ __global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan,
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan, uint32_t level,
+    const T* __restrict__ vals, const uint32_t* __restrict__ inv, uint32_t* __restrict__ owner,
+    uint4* __restrict__ state, uint32_t* control) {
+    level_walk_run<T>(launch_grid(), plan, level, vals, inv, owner, state, control);
+}
+
 // Cycles no ruler reached (both orbits ruler-free): thread per pair-node
 // whose two vertices are unowned.  Only the walker starting at the smallest
 // even vertex of its orbit walks the orbit whole (the others stop at the
@@ -223,15 +230,15 @@ __global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan,
 // one of the two orbits, so every pair-node of the cycle gets a stamped
 // colour; the cost is O(L log L) per cycle.
 template <typename T>
-__global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ vals, const uint32_t* __restrict__ inv,
     uint32_t* __restrict__ owner, uint32_t* control) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t total = (uint64_t)pcap << level;
-    for (uint64_t pidx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; pidx < total;
-         pidx += (uint64_t)gridDim.x * blockDim.x) {
+    for (uint64_t pidx = (uint64_t)grid.bid * blockDim.x + threadIdx.x; pidx < total;
+         pidx += (uint64_t)grid.nblk * blockDim.x) {
         const uint32_t j = (uint32_t)(pidx / pcap);
         const uint32_t k = (uint32_t)(pidx - (uint64_t)j * pcap);
         const uint32_t s = size_at(lv, level, j);
@@ -285,12 +292,19 @@ __global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__
     }
 }
 
+template <typename T>
+__global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ vals, const uint32_t* __restrict__ inv,
+    uint32_t* __restrict__ owner, uint32_t* control) {
+    level_walk_short_run<T>(launch_grid(), plan, level, vals, inv, owner, control);
+}
+
 // One pointer-jumping round over ruler states (src -> dst).  Blocks claim
 // chunks of rulers in address order, so the rulers being jumped at any time
 // (and, early on, the near successors they read) stay close together.
 // The done/hard words were written by earlier launches, so every thread of
 // a block sees the same value and the block leaves together.
-__global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
+__device__ __forceinline__ void ruler_jump_run(Grid grid, const uint4* __restrict__ src,
     uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
         *(volatile uint32_t*)(control + kCtlHard) != 0) {
@@ -322,9 +336,14 @@ __global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
     (void)round;
 }
 
+__global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
+    uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
+    ruler_jump_run(launch_grid(), src, dst, rulers, round, control);
+}
+
 // After a round: a round that changed nothing means every ruler holds its
 // orbit's minima; later rounds then return at once.
-__global__ void ruler_check(uint32_t round, uint32_t* control) {
+__device__ __forceinline__ void ruler_check_run(Grid grid, uint32_t round, uint32_t* control) {
     control[kCtlClaimJump] = 0; // the next round claims from the start again
     if (control[kCtlDone] != 0 || control[kCtlHard] != 0) {
         return;
@@ -334,6 +353,10 @@ __global__ void ruler_check(uint32_t round, uint32_t* control) {
         control[kCtlDone] = 1;
     }
     control[kCtlChanged] = 0;
+}
+
+__global__ void ruler_check(uint32_t round, uint32_t* control) {
+    ruler_check_run(launch_grid(), round, control);
 }
 
 // Levels with few super-rulers spend their jumping time on launches, not on
@@ -351,7 +374,7 @@ constexpr uint32_t kJumpBlockBatch = 4;
 #endif
 constexpr uint32_t kJumpBlockMaxStates = 1u << BPB200_JUMP_BLOCK_LOG2;
 
-__global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* s0, uint4* s1,
+__device__ __forceinline__ void ruler_jump_block_run(Grid grid, uint4* s0, uint4* s1,
     uint32_t supers, uint32_t rounds, uint32_t* control) {
     // written by earlier launches: every thread reads the same values
     if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
@@ -428,6 +451,11 @@ __global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* 
     }
 }
 
+__global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* s0, uint4* s1,
+    uint32_t supers, uint32_t rounds, uint32_t* control) {
+    ruler_jump_block_run(launch_grid(), s0, s1, supers, rounds, control);
+}
+
 // ---------------------------------------------------------------------------
 // Super-rulers.  Jumping over all rulers costs a full pass over their states
 // per round (about log2 of the rulers in an orbit rounds).  Instead every
@@ -440,7 +468,7 @@ __global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* 
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSuperLog2 = 4;
 
-__global__ void __launch_bounds__(256) ruler_super_walk(const uint4* __restrict__ state,
+__device__ __forceinline__ void ruler_super_walk_run(Grid grid, const uint4* __restrict__ state,
     uint32_t rulers, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
     uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
@@ -476,16 +504,22 @@ __global__ void __launch_bounds__(256) ruler_super_walk(const uint4* __restrict_
     }
 }
 
+__global__ void __launch_bounds__(256) ruler_super_walk(const uint4* __restrict__ state,
+    uint32_t rulers, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
+    uint32_t* control) {
+    ruler_super_walk_run(launch_grid(), state, rulers, sstate, super_of, control);
+}
+
 // Ruler cycles that contain no super-ruler: thread per ruler no super walk
 // reached; the ruler with the smallest id of its cycle folds the cycle's
 // minima and stamps the colour on every ruler of it.
-__global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict__ state,
+__device__ __forceinline__ void ruler_super_short_run(Grid grid, const uint4* __restrict__ state,
     uint32_t rulers, uint32_t* __restrict__ super_of, uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
         return;
     }
-    for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rulers;
-         r += gridDim.x * blockDim.x) {
+    for (uint32_t r = grid.bid * blockDim.x + threadIdx.x; r < rulers;
+         r += grid.nblk * blockDim.x) {
         if (super_of[r] != kUnset) {
             continue;
         }
@@ -532,12 +566,21 @@ __global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict
     }
 }
 
+__global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict__ state,
+    uint32_t rulers, uint32_t* __restrict__ super_of, uint32_t* control) {
+    ruler_super_short_run(launch_grid(), state, rulers, super_of, control);
+}
+
 // Clears the level's control words; `force_union_find` pre-sets the hard
 // flag so the level is coloured by union-find (a test hook for that path).
-__global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
+__device__ __forceinline__ void control_reset_run(Grid grid, uint32_t* control, uint32_t force_union_find) {
     if (threadIdx.x < kCtlWords) {
         control[threadIdx.x] = threadIdx.x == kCtlHard ? force_union_find : 0u;
     }
+}
+
+__global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
+    control_reset_run(launch_grid(), control, force_union_find);
 }
 
 // Colours (from the walks, or from union-find when the level fell back),
@@ -546,7 +589,7 @@ __global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
 // stay within the nodes it covers.  Every thread of a block runs every
 // claimed chunk (the colour bitmap is assembled with warp shuffles).
 template <typename T>
-__global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
+__device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
     const uint32_t* __restrict__ super_of, const uint4* __restrict__ state0,
     const uint4* __restrict__ state1, uint32_t* uf,
@@ -569,7 +612,7 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
     // components, which then serialise: those stride over the whole level
     // (at 2^30 uniform entries, claimed order took 18.5 -> 12.5 ms on the
     // 2^30-slot level but 14 -> 19 ms on 2^24-slot nodes).
-    uint64_t first = (uint64_t)blockIdx.x * chunk;
+    uint64_t first = (uint64_t)grid.bid * chunk;
     bool started = false;
     const bool claimed = !hard || cap > (1ull << BPB200_FINAL_STRIDE_LOG2);
     auto next_chunk = [&]() -> bool {
@@ -577,7 +620,7 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
             return claim_chunk(control + kCtlClaimFinal, chunk, total, &first);
         }
         if (started) {
-            first += (uint64_t)gridDim.x * chunk;
+            first += (uint64_t)grid.nblk * chunk;
         }
         started = true;
         return first < total;
@@ -682,6 +725,16 @@ __global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ p
             xbits[p0 >> 5] = v;
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
+    uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
+    const uint32_t* __restrict__ super_of, const uint4* __restrict__ state0,
+    const uint4* __restrict__ state1, uint32_t* uf,
+    uint32_t* __restrict__ xbits, uint32_t* __restrict__ dst, uint32_t* control,
+    uint32_t* status) {
+    level_finalize_run<T>(launch_grid(), plan, level, src, owner, super_of, state0, state1, uf, xbits, dst, control, status);
 }
 
 } // namespace bpb200

@@ -184,3 +184,65 @@ def test_stream240_plain_batch_and_server_match_reference(gpu):
         for t, w in zip(tickets, want):
             blob, latency = server.wait(t)
             assert _digest(blob) == w and latency > 0
+
+
+def _device_items(gpu, torch, reqs):
+    items, keep = [], []
+    for perm, fmt in reqs:
+        n, width = perm.size, perm.dtype.itemsize
+        size = gpu.encoded_size(n, fmt)
+        d_in = torch.from_numpy(perm.view(np.int64 if width == 8 else np.int32)).cuda()
+        d_blob = torch.full(((size + 3) // 4 * 4,), 0x3C, dtype=torch.uint8, device="cuda")
+        keep.append((d_in, d_blob, size))
+        items.append((d_in.data_ptr(), n, width, fmt, d_blob.data_ptr(), size))
+    return items, keep
+
+
+def test_batch_groups_few_launches_and_union_find(gpu):
+    """Mid-size requests (above one tile, up to the walk limit) are encoded
+    together, level by level, by the batched level kernels: far fewer
+    launches than one level chain per request, and the same bytes as the
+    plain call, with the orbit walks and with union-find forced."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(77)
+    reqs = []
+    for i in range(48):
+        n = int(rng.integers(8193, 1 << 18))
+        dtype = np.uint64 if i % 3 == 0 else np.uint32
+        perm = gpu.fill_permutation(gpu.PermutationKind(i % 2), 500 + i, n, dtype)
+        fmt = gpu.FormatOptions(middle_group_log2=4 + i % 2,
+                                middle_placement=gpu.MiddlePlacement(i % 3))
+        reqs.append((perm, fmt))
+    for uf in (False, True):
+        gpu.set_union_find_only(uf)
+        try:
+            want = [gpu.compress(p, gpu.CompressOptions(format=f)) for p, f in reqs]
+            items, keep = _device_items(gpu, torch, reqs)
+            statuses, launches = gpu.compress_batch_device(items)
+            torch.cuda.synchronize()
+        finally:
+            gpu.set_union_find_only(False)
+        assert statuses == [0] * len(reqs)
+        assert launches < 4 * len(reqs), launches  # a level chain alone is ~50-100
+        for (_, d_blob, size), w in zip(keep, want):
+            assert d_blob[:size].cpu().numpy().tobytes() == w
+
+
+def test_batch_group_member_with_duplicate(gpu, oracle):
+    """A non-permutation inside a group fails alone: it reports
+    invalid_argument and every other member keeps its exact bytes."""
+    torch = pytest.importorskip("torch")
+    reqs = []
+    for i, n in enumerate((20000, 70001, 150000, 9000, 33333)):
+        perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 900 + i, n)
+        reqs.append((perm, gpu.FormatOptions()))
+    bad = reqs[2][0].copy()
+    bad[5] = bad[77]
+    reqs[2] = (bad, reqs[2][1])
+    items, keep = _device_items(gpu, torch, reqs)
+    statuses, _ = gpu.compress_batch_device(items, raise_errors=False)
+    torch.cuda.synchronize()
+    assert statuses == [0, 0, 1, 0, 0]
+    for k, ((_, d_blob, size), (perm, _)) in enumerate(zip(keep, reqs)):
+        if k != 2:
+            assert d_blob[:size].cpu().numpy().tobytes() == oracle.compress(perm)

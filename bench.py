@@ -75,7 +75,9 @@ def parse_args():
                     help="reference arm: also time one full 2^30 compress (minutes)")
     ap.add_argument("--workload", default="headline", choices=("headline", "serving"),
                     help="serving: the mixed-size request stream (not the headline metric)")
-    ap.add_argument("--requests", type=int, default=1024, help="serving: number of requests")
+    ap.add_argument("--requests", type=int, default=4096, help="serving: number of requests")
+    ap.add_argument("--no-serving", action="store_true",
+                    help="headline run without the serving sub-object")
     ap.add_argument("--max-log2", type=int, default=24, help="serving: largest log2 N")
     ap.add_argument("--hbm-budget", type=int, default=120 * 10**9, help="serving: admission budget")
     ap.add_argument("--workers", type=int, default=4,
@@ -495,6 +497,12 @@ def b200_arm(args, world, rank, local):
     }
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
+    if world == 1 and not args.no_serving:
+        # the serving stream runs after the headline's buffers are released
+        del d_in, d_blob, host, host_blob, perm, blob_np
+        torch.cuda.empty_cache()
+        bp.shutdown()
+        line["serving"] = serving_run(args)
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -557,9 +565,27 @@ def _section_bits(n, fmt):
     return sizes(n)
 
 
-def serving_arm(args):
-    """Mixed-size request stream: plain per-request calls, then the serving
-    loop with Poisson arrivals at 1.5x the plain path's request rate."""
+def stream_digests(requests, max_log2):
+    """The reference's per-request SHA-256 prefixes (hex, 128 bits) for the
+    mixed stream, from tests/golden/reference_digests.json, or None."""
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", "reference_digests.json")) as f:
+            d = json.load(f)["stream4096"]
+    except (OSError, KeyError, ValueError):
+        return None
+    if d["seed"] != SEED or d["max_log2"] != max_log2 or d["requests"] < requests:
+        return None
+    return d["sha256_128"][:requests]
+
+
+def serving_run(args):
+    """Mixed-size request stream (the fifth configuration): plain
+    per-request calls (bpb200_compress one after another), then the serving
+    loop twice: every request submitted at once (capacity) and Poisson
+    arrivals at 1.5x the plain path's request rate (paced).  Every blob of
+    every run is compared with the plain call's and, where the committed
+    reference digests cover the stream, with the reference's own bytes.
+    Returns the record (host wall clock, submit to blob in host memory)."""
     import concurrent.futures as futures
     import hashlib
     import threading
@@ -582,13 +608,14 @@ def serving_arm(args):
     for p, o in zip(perms[:8], opts[:8]):                # warm-up
         bp.compress(p, o)
 
-    # plain per-request calls; the byte check (sha256) runs after the timing
+    # plain per-request calls; the byte checks run after the timing
     t0 = time.perf_counter()
     plain_blobs = [bp.compress(p, o) for p, o in zip(perms, opts)]
     t_plain = time.perf_counter() - t0
     plain_rate = total / t_plain
-    plain = [hashlib.sha256(b).digest() for b in plain_blobs]
+    plain = [hashlib.sha256(b).hexdigest()[:32] for b in plain_blobs]
     del plain_blobs
+    want = stream_digests(len(perms), args.max_log2)
 
     def serve(arrivals):
         """Runs the stream through a server; arrivals (seconds from the start,
@@ -621,18 +648,18 @@ def serving_arm(args):
         th.join()
         stats = server.stats()
         server.close()
-        same = all(hashlib.sha256(b).digest() == h for b, h in zip(blobs, plain))
-        return t_serve, np.sort(np.array(latencies)), same, stats
+        got = [hashlib.sha256(b).hexdigest()[:32] for b in blobs]
+        return t_serve, np.sort(np.array(latencies)), got, stats
 
     # capacity: every request submitted at once (offered load above capacity)
-    t_serve, lat, identical, stats = serve(None)
-    # latency under the stated offered load: Poisson arrivals at 1.5x the
-    # plain path's request rate
+    t_serve, lat, got, stats = serve(None)
+    # latency under the stated offered load
     rate = 1.5 * len(perms) / t_plain                    # offered load, requests/s
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(perms)))
-    t_paced, lat_paced, identical_paced, _ = serve(arrivals)
-    identical = identical and identical_paced
-    line = {
+    t_paced, lat_paced, got_paced, _ = serve(arrivals)
+    identical = got == plain and got_paced == plain
+    ref_match = None if want is None else (plain == want and got == want and got_paced == want)
+    return {
         "metric": "entries/s on the mixed-size serving stream (serving loop vs plain per-request)",
         "value": total / t_serve, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
         "plain_per_request": plain_rate, "ratio_vs_plain": (total / t_serve) / plain_rate,
@@ -645,7 +672,10 @@ def serving_arm(args):
                   "p50_latency_s": float(np.percentile(lat_paced, 50)),
                   "p99_latency_s": float(np.percentile(lat_paced, 99))},
         "identical_bytes": bool(identical),
-        "kernel_launches": stats["kernel_launches"], "workers": args.workers, "data": "synthetic",
+        "reference_sha256_match": ref_match,
+        "kernel_launches": stats["kernel_launches"],
+        "launches_per_request": stats["kernel_launches"] / len(perms),
+        "workers": args.workers, "data": "synthetic",
         "config": {"workload": f"{len(perms)} requests, N = round(2^U(10,{args.max_log2})), "
                                "Fisher-Yates or Sattolo, uint32 or uint64, m in {4,5}, "
                                "placement uniform over 3, default clusters; capacity run with "
@@ -654,7 +684,10 @@ def serving_arm(args):
                    "timing": "host wall clock (submit to blob in host memory); byte checks "
                              "after the timed runs"},
     }
-    print(json.dumps(line), flush=True)
+
+
+def serving_arm(args):
+    print(json.dumps(serving_run(args)), flush=True)
 
 
 def main():

@@ -35,12 +35,13 @@ __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pa
     uint32_t o = 0;
     off[0] = o; o = align_up(o + slots * 2, 16);           // vals[0]
     off[1] = o; o = align_up(o + slots * 2, 16);           // vals[1]
-    off[2] = o; o = align_up(o + slots * 2, 16);           // inv
+    off[2] = o; o = align_up(o + slots * 2, 16);           // inv[0]
     off[3] = o; o = align_up(o + pairs * 4, 16);           // uf
     off[4] = o; o = align_up(o + words * 4, 16);           // xbits (input switches)
     off[5] = o; o = align_up(o + words * 4, 16);           // ybits (output switches)
     off[6] = o; o = align_up(o + 2 * kNodeWave * (uint32_t)sizeof(NodeAddress), 16);
     off[7] = o; o = align_up(o + kNodeWave * 8, 16);       // leafbit
+    off[8] = o; o = align_up(o + slots * 2, 16);           // inv[1]
     return o;
 }
 
@@ -48,10 +49,10 @@ template <typename T>
 __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
     uint32_t pairs, uint32_t tile, unsigned char* smem) {
-    uint32_t off[8];
+    uint32_t off[9];
     tile_smem_layout(slots, pairs, off);
     uint16_t* vals[2] = {(uint16_t*)(smem + off[0]), (uint16_t*)(smem + off[1])};
-    uint16_t* inv = (uint16_t*)(smem + off[2]);
+    uint16_t* invs[2] = {(uint16_t*)(smem + off[2]), (uint16_t*)(smem + off[8])};
     uint32_t* uf = (uint32_t*)(smem + off[3]);
     uint32_t* xbits = (uint32_t*)(smem + off[4]);
     uint32_t* ybits = (uint32_t*)(smem + off[5]);
@@ -97,6 +98,8 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
         const uint32_t first = J << t;
         uint16_t* cur = vals[t & 1];
         uint16_t* nxt = vals[(t + 1) & 1];
+        uint16_t* inv = invs[t & 1];        // this level's inverse
+        uint16_t* child_inv = invs[(t + 1) & 1];
         // uniform per level: whether every node here exists / is internal
         const bool all_exist = level == 0 || plan.levels[level - 1].q > leaf;
         const bool all_internal = lv.q > leaf && all_exist;
@@ -115,8 +118,10 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 }
                 __syncthreads();
             }
-            // A: inverse and union-find init
-            for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
+            // A (first tile level only; every later level's inverse and
+            // union-find roots come from its parent's phase E0): inverse
+            // and union-find init
+            for (uint32_t e = tid; t == 0 && e < nodes * cap; e += blockDim.x) {
                 const uint32_t path = by_cap(e);
                 const uint32_t i = e - path * cap;
                 const uint32_t s = size_at(lv, level, first + path);
@@ -203,7 +208,11 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 }
             }
             __syncthreads();
-            // E0: output switch bits in natural order
+            // E0: output switch bits in natural order, and the children's
+            // inverse and union-find roots (as level_outputs does for the
+            // global levels: output pair k's colour-0 input inv[2k + y]
+            // goes left with value k, the other right)
+            const uint32_t ccpcap = (uint32_t)plan.levels[level + 1].pcap;
             for (uint32_t base = warp * 32; base < ptotal; base += nwarps * 32) {
                 const uint32_t p = base + lane;
                 bool y = false;
@@ -211,11 +220,35 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     const uint32_t path = by_pcap(p);
                     const uint32_t k = p - path * pcap;
                     const uint32_t s = size_at(lv, level, first + path);
-                    if (k < s / 2 && internal_node(path, s)) {
-                        const uint32_t u = inv[path * cap + 2 * k];
-                        if (u < s) { // an unwritten slot (repeated value) holds anything
-                            const uint32_t q = path * pcap + (u >> 1);
-                            y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                    const uint32_t half = s / 2;
+                    if (k <= half && internal_node(path, s)) {
+                        const uint32_t lb = 2 * path * ccap;
+                        const uint32_t rb = lb + ccap;
+                        if (k < half) {
+                            const uint32_t u = inv[path * cap + 2 * k];
+                            const uint32_t w = inv[path * cap + 2 * k + 1];
+                            uint16_t to_left = 0xffffu, to_right = 0xffffu;
+                            if (u < s && w < s) { // an unwritten slot (repeated value) holds anything
+                                const uint32_t q = path * pcap + (u >> 1);
+                                y = (((xbits[q >> 5] >> (q & 31)) ^ u) & 1u) != 0;
+                                to_left = (uint16_t)((y ? w : u) >> 1);
+                                to_right = (uint16_t)((y ? u : w) >> 1);
+                            }
+                            child_inv[lb + k] = to_left;
+                            child_inv[rb + k] = to_right;
+                        } else if ((s & 1u) != 0) {
+                            const uint32_t u = inv[path * cap + s - 1];
+                            child_inv[lb + half] = u < s ? (uint16_t)(u >> 1) : (uint16_t)0xffffu;
+                        }
+                        if ((k & 1u) == 0) {
+                            if (k < s - half) {
+                                const uint32_t id = 2 * path * ccpcap + (k >> 1);
+                                uf[id] = id << 1;
+                            }
+                            if (k < half) {
+                                const uint32_t id = (2 * path + 1) * ccpcap + (k >> 1);
+                                uf[id] = id << 1;
+                            }
                         }
                     }
                 }

@@ -315,6 +315,39 @@ def last_profile_launches():
     return [(KERNEL_KINDS[kinds[i]], levels[i], secs[i]) for i in range(n)]
 
 
+class Tuning(ctypes.Structure):
+    """Launch choices of one size class (bpb200_tuning); none changes bytes."""
+    _fields_ = [("walk_blocks_per_sm", ctypes.c_uint32), ("walk_max_log2", ctypes.c_uint32),
+                ("jump_block_log2", ctypes.c_uint32), ("tile_max_log2", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
+def get_tuning(count: int) -> dict:
+    """The setting calls with ``count`` entries use (table or forced)."""
+    lib = library()
+    lib.bpb200_get_tuning.argtypes = [ctypes.c_uint64, ctypes.POINTER(Tuning)]
+    t = Tuning()
+    raise_for(lib.bpb200_get_tuning(count, ctypes.byref(t)), "invalid tuning query")
+    return t.as_dict()
+
+
+def set_tuning(setting: Optional[dict]) -> None:
+    """Forces ``setting`` (a dict of Tuning fields; missing ones take the
+    current table's value for 2^20 entries) for every later call, or returns
+    to the table with None."""
+    lib = library()
+    lib.bpb200_set_tuning.argtypes = [ctypes.POINTER(Tuning)]
+    if setting is None:
+        lib.bpb200_set_tuning(None)
+        return
+    base = get_tuning(1 << 20)
+    base.update(setting)
+    t = Tuning(**base)
+    lib.bpb200_set_tuning(ctypes.byref(t))
+
+
 def describe(count: int, fmt: Optional[FormatOptions] = None):
     """(routing depth, first tile level) of the encode for (count, fmt)."""
     cf = to_c_format(fmt)

@@ -16,6 +16,7 @@
 #include "walk.cuh"
 
 #include <cuda_runtime.h>
+#include <dlfcn.h>
 
 #include <algorithm>
 #include <atomic>
@@ -244,11 +245,11 @@ TileShape tile_shape(const Plan& p, uint32_t t0) {
     return s;
 }
 
-// Picks the tile level: the first level whose nodes fit a tile whose
-// deepest padded level also fits the shared-memory budget.
-void choose_tile(Plan& p, TileShape* shape) {
+// Picks the tile level: the first level whose nodes fit `tile_max` entries
+// and whose deepest padded tile level also fits the shared-memory budget.
+void choose_tile(Plan& p, TileShape* shape, uint64_t tile_max = kTileMaxEntries) {
     uint32_t t0 = 0;
-    while (t0 < p.depth && p.levels[t0].cap > kTileMaxEntries) {
+    while (t0 < p.depth && p.levels[t0].cap > tile_max) {
         ++t0;
     }
     TileShape s = tile_shape(p, t0);
@@ -269,16 +270,135 @@ void choose_tile(Plan& p, TileShape* shape) {
 
 std::atomic<int> g_force_union_find{0};
 
-// Launch-shape tuning (BPB200_WALK_BLOCKS_PER_SM overrides the default):
-// resident walkers times the slots per ruler is the address window the
-// walks keep live, which must stay inside L2.
-int walk_blocks_per_sm() {
-    static const int value = [] {
+// ------------------------------------------------------------ tuning
+//
+// Launch choices that change speed but never bytes, per size class (the
+// class of a permutation of n entries is ceil(log2 n)):
+//   walk_blocks_per_sm  persistent level_walk blocks per SM; resident
+//                       walkers times the slots per ruler is the address
+//                       window the walks keep live, which must stay in L2
+//   walk_max_log2       largest node coloured by orbit walks (larger nodes
+//                       by union-find); at most the compiled walk limit
+//   jump_block_log2     largest super-ruler count whose pointer-jumping
+//                       rounds run inside one CTA (else one launch pair per
+//                       round)
+//   tile_max_log2       largest node handed to the shared-memory tile
+// The table comes from tuning.json beside this library (written by
+// benes_perm_b200/tune.py; BPB200_TUNING_FILE names another file, "none"
+// disables it), loaded once; classes it lacks take the nearest class it
+// has, and without a table the compiled defaults apply.
+// BPB200_WALK_BLOCKS_PER_SM overrides the default walk blocks per SM.
+struct Tuning {
+    uint32_t walk_blocks_per_sm;
+    uint32_t walk_max_log2;
+    uint32_t jump_block_log2;
+    uint32_t tile_max_log2;
+};
+
+Tuning default_tuning() {
+    static const Tuning t = [] {
         const char* env = std::getenv("BPB200_WALK_BLOCKS_PER_SM");
         const int v = env ? std::atoi(env) : 4;
-        return v < 1 ? 1 : (v > 8 ? 8 : v);
+        return Tuning{(uint32_t)(v < 1 ? 1 : (v > 8 ? 8 : v)), BPB200_WALK_MAX_LOG2,
+            BPB200_JUMP_BLOCK_LOG2, 13};
     }();
-    return value;
+    return t;
+}
+
+Tuning clamp_tuning(Tuning t) {
+    auto clamp = [](uint32_t v, uint32_t lo, uint32_t hi) { return v < lo ? lo : (v > hi ? hi : v); };
+    t.walk_blocks_per_sm = clamp(t.walk_blocks_per_sm, 1, 8);
+    t.walk_max_log2 = clamp(t.walk_max_log2, 10, BPB200_WALK_MAX_LOG2);
+    t.jump_block_log2 = clamp(t.jump_block_log2, 4, 18);
+    t.tile_max_log2 = clamp(t.tile_max_log2, 9, 13);
+    return t;
+}
+
+struct TuningTable {
+    bool has[64] = {};
+    Tuning at[64];
+};
+
+// Reads {"classes": {"<class>": {"<knob>": <int>, ...}, ...}}; anything
+// else in the file is ignored.  A missing or malformed file gives an empty
+// table.
+TuningTable load_tuning_table() {
+    TuningTable t;
+    std::string path;
+    if (const char* env = std::getenv("BPB200_TUNING_FILE")) {
+        path = env;
+    } else {
+        Dl_info info{};
+        if (dladdr((void*)&default_tuning, &info) != 0 && info.dli_fname != nullptr) {
+            path = info.dli_fname;
+            const size_t slash = path.find_last_of('/');
+            path = (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) +
+                "/tuning.json";
+        }
+    }
+    if (path.empty() || path == "none") return t;
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (f == nullptr) return t;
+    std::string text;
+    char buf[4096];
+    size_t got;
+    while ((got = std::fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, got);
+    std::fclose(f);
+    size_t at = text.find("\"classes\"");
+    if (at == std::string::npos) return t;
+    at = text.find('{', at);
+    while (at != std::string::npos) {
+        const size_t q0 = text.find('"', at + 1);
+        const size_t close = text.find('}', at + 1);
+        if (q0 == std::string::npos || (close != std::string::npos && close < q0)) break;
+        const size_t q1 = text.find('"', q0 + 1);
+        const size_t open = text.find('{', q1);
+        const size_t end = text.find('}', open);
+        if (q1 == std::string::npos || open == std::string::npos || end == std::string::npos) break;
+        const int cls = std::atoi(text.substr(q0 + 1, q1 - q0 - 1).c_str());
+        Tuning v = default_tuning();
+        const std::string body = text.substr(open + 1, end - open - 1);
+        auto knob = [&](const char* name, uint32_t* field) {
+            const size_t k = body.find(std::string("\"") + name + "\"");
+            if (k == std::string::npos) return;
+            const size_t colon = body.find(':', k);
+            if (colon != std::string::npos) *field = (uint32_t)std::atoi(body.c_str() + colon + 1);
+        };
+        knob("walk_blocks_per_sm", &v.walk_blocks_per_sm);
+        knob("walk_max_log2", &v.walk_max_log2);
+        knob("jump_block_log2", &v.jump_block_log2);
+        knob("tile_max_log2", &v.tile_max_log2);
+        if (cls >= 0 && cls < 64) {
+            t.has[cls] = true;
+            t.at[cls] = clamp_tuning(v);
+        }
+        at = end;
+    }
+    return t;
+}
+
+std::mutex g_tuning_mutex;
+bool g_tuning_forced = false;
+Tuning g_tuning_force{};
+
+uint32_t size_class(uint64_t n) {
+    uint32_t c = 0;
+    while (c < 63 && (1ull << c) < n) ++c;
+    return c;
+}
+
+Tuning tuning_for(uint64_t count) {
+    static const TuningTable table = load_tuning_table();
+    {
+        std::lock_guard<std::mutex> lock(g_tuning_mutex);
+        if (g_tuning_forced) return g_tuning_force;
+    }
+    const int c = (int)size_class(count);
+    for (int d = 0; d < 64; ++d) {
+        if (c - d >= 0 && table.has[c - d]) return table.at[c - d];
+        if (c + d < 64 && table.has[c + d]) return table.at[c + d];
+    }
+    return default_tuning();
 }
 
 int grid_for(uint64_t work, int threads) {
@@ -384,8 +504,9 @@ void emission_launches(const Plan& p, uint32_t l, int side, F&& f) {
 // inverse; `child_inv` receives the next level's (null when the next level
 // is the tile's, which builds its own in shared memory).
 template <typename TV>
-void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint32_t l,
-    const TV* src, uint32_t* dst, uint32_t* d_blob, uint32_t* inv, uint32_t* child_inv) {
+void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, const Tuning& tune,
+    uint32_t l, const TV* src, uint32_t* dst, uint32_t* d_blob, uint32_t* inv,
+    uint32_t* child_inv) {
     const Plan* dp = w.d_plan;
     const LevelInfo& lv = p.levels[l];
     const uint64_t slots = lv.cap << l;
@@ -400,7 +521,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
     const int gw = grid_for(buckets, kLevelThreads);
     uint32_t* ctl = w.control;
     // nodes whose arrays do not fit in L2 are coloured by union-find
-    const bool walks = lv.cap <= kWalkMaxNode && g_force_union_find.load() == 0;
+    const bool walks = lv.cap <= (1ull << tune.walk_max_log2) && g_force_union_find.load() == 0;
     control_reset<<<1, 32, 0, st>>>(ctl, walks ? 0u : 1u);
     rec.launches += 1;
     if (l == 0 && lv.cap > kWalkMaxNode && w.records != nullptr) {
@@ -430,7 +551,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             const uint64_t want = ((uint64_t)buckets + kWalkChunk - 1) / kWalkChunk * 32;
             const int gwalk = (int)std::max<uint64_t>(1,
-                std::min<uint64_t>((uint64_t)sms * walk_blocks_per_sm(),
+                std::min<uint64_t>((uint64_t)sms * tune.walk_blocks_per_sm,
                     (want + kLevelThreads - 1) / kLevelThreads));
             level_walk<TV><<<gwalk, kLevelThreads, 0, st>>>(dp, l, src, inv, w.owner,
                 w.state[0], ctl);
@@ -445,7 +566,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, uint
         }
         uint4* sstate[2] = {w.state[1], w.state[1] + supers};
         // few super-rulers: every round in one CTA; otherwise one launch pair per round
-        const bool one_block = supers <= kJumpBlockMaxStates;
+        const bool one_block = supers <= (1u << tune.jump_block_log2);
         rec.launch(kKindJump, [&] {
             check(cudaMemsetAsync(w.super_of, 0xff, (uint64_t)buckets * 4, st),
                 "cudaMemsetAsync(super rulers)");
@@ -535,7 +656,7 @@ void allow_tile_smem(const void* kernel) {
 
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
-    const TileShape& shape, const T* d_in, uint32_t* d_blob) {
+    const TileShape& shape, const Tuning& tune, const T* d_in, uint32_t* d_blob) {
     const Plan* dp = w.d_plan;
     const uint32_t t0 = p.tile_level;
     if (t0 > 0) {
@@ -550,9 +671,10 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         uint32_t* dst = w.vals[l & 1];
         uint32_t* child_inv = l + 1 < t0 ? invs[(l + 1) & 1] : nullptr;
         if (l == 0) {
-            run_level<T>(w, rec, st, p, l, d_in, dst, d_blob, invs[0], child_inv);
+            run_level<T>(w, rec, st, p, tune, l, d_in, dst, d_blob, invs[0], child_inv);
         } else {
-            run_level<uint32_t>(w, rec, st, p, l, cur32, dst, d_blob, invs[l & 1], child_inv);
+            run_level<uint32_t>(w, rec, st, p, tune, l, cur32, dst, d_blob, invs[l & 1],
+                child_inv);
         }
         cur32 = dst;
     }
@@ -581,6 +703,7 @@ struct Call {
     Layout layout;
     Plan* plan = nullptr;
     TileShape shape{};
+    Tuning tune{};
 };
 
 void set_error(char* err, size_t len, const std::string& msg) {
@@ -621,8 +744,10 @@ int check_device_buffers(const void* d_entries, uint32_t entry_bytes, const void
 }
 
 // Validation shared by both entry points; fills the layout and plan.
+// `tune` (null: the table's setting for `count`) fixes the tile size.
 int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
-    uint64_t blob_len, Workspace& w, Call* call, char* err, size_t err_len) {
+    uint64_t blob_len, Workspace& w, Call* call, char* err, size_t err_len,
+    const Tuning* tune = nullptr) {
     if (entry_bytes != 4 && entry_bytes != 8) {
         set_error(err, err_len, "entry width must be 4 or 8 bytes");
         return kInvalidArgument;
@@ -649,12 +774,14 @@ int prepare(uint64_t count, uint32_t entry_bytes, const bpb200_format* format,
         return kLength;
     }
     call->plan = w.h_plan;
-    e = make_plan(call->layout, kTileMaxEntries, call->plan);
+    call->tune = tune != nullptr ? *tune : tuning_for(count);
+    const uint64_t tile_max = 1ull << call->tune.tile_max_log2;
+    e = make_plan(call->layout, tile_max, call->plan);
     if (!e.ok()) {
         set_error(err, err_len, e.message);
         return e.code;
     }
-    choose_tile(*call->plan, &call->shape);
+    choose_tile(*call->plan, &call->shape, tile_max);
     if (call->shape.smem > kTileSmemBudget) {
         set_error(err, err_len, "tile does not fit in shared memory");
         return kLength;
@@ -689,9 +816,11 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     check(cudaMemsetAsync(d_blob, 0, (p.end_offset + 3) / 4 * 4, st), "cudaMemsetAsync(blob)");
     rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h); });
     if (entry_bytes == 4) {
-        launch_levels<uint32_t>(w, rec, st, p, call.shape, (const uint32_t*)d_in, d_blob);
+        launch_levels<uint32_t>(w, rec, st, p, call.shape, call.tune, (const uint32_t*)d_in,
+            d_blob);
     } else {
-        launch_levels<uint64_t>(w, rec, st, p, call.shape, (const uint64_t*)d_in, d_blob);
+        launch_levels<uint64_t>(w, rec, st, p, call.shape, call.tune, (const uint64_t*)d_in,
+            d_blob);
     }
     check(cudaEventRecord(w.stop, st), "cudaEventRecord");
     check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
@@ -908,6 +1037,26 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
 
 void bpb200_set_profiling(int enabled) { g_profiling.store(enabled ? 1 : 0); }
 
+int bpb200_get_tuning(uint64_t count, bpb200_tuning* out) {
+    if (out == nullptr) return kInvalidArgument;
+    const Tuning t = tuning_for(count);
+    out->walk_blocks_per_sm = t.walk_blocks_per_sm;
+    out->walk_max_log2 = t.walk_max_log2;
+    out->jump_block_log2 = t.jump_block_log2;
+    out->tile_max_log2 = t.tile_max_log2;
+    return kOk;
+}
+
+int bpb200_set_tuning(const bpb200_tuning* forced) {
+    std::lock_guard<std::mutex> lock(g_tuning_mutex);
+    g_tuning_forced = forced != nullptr;
+    if (forced != nullptr) {
+        g_tuning_force = clamp_tuning(Tuning{forced->walk_blocks_per_sm, forced->walk_max_log2,
+            forced->jump_block_log2, forced->tile_max_log2});
+    }
+    return kOk;
+}
+
 void bpb200_set_colouring(int union_find_only) { g_force_union_find.store(union_find_only ? 1 : 0); }
 
 int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth,
@@ -918,11 +1067,12 @@ int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth
         return e.code;
     }
     std::unique_ptr<Plan> p(new Plan);
-    if (!make_plan(L, kTileMaxEntries, p.get()).ok()) {
+    const uint64_t tile_max = 1ull << tuning_for(count).tile_max_log2;
+    if (!make_plan(L, tile_max, p.get()).ok()) {
         return kLength;
     }
     TileShape shape;
-    choose_tile(*p, &shape);
+    choose_tile(*p, &shape, tile_max);
     if (depth) *depth = p->depth;
     if (tile_level) *tile_level = p->tile_level;
     return kOk;
@@ -1104,7 +1254,8 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         Workspace w; // views into the static array; owns nothing
         w.h_plan = &noalloc::g_plan;
         Call call;
-        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+        const Tuning fixed = default_tuning(); // the scratch limits assume the compiled tile size
+        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len, &fixed);
         if (rc != kOk) {
             return rc;
         }
@@ -1147,10 +1298,10 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
         rec.st = st;
         rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, (uint32_t*)d_blob, h); });
         if (entry_bytes == 4) {
-            launch_levels<uint32_t>(w, rec, st, p, call.shape, (const uint32_t*)d_entries,
+            launch_levels<uint32_t>(w, rec, st, p, call.shape, call.tune, (const uint32_t*)d_entries,
                 (uint32_t*)d_blob);
         } else {
-            launch_levels<uint64_t>(w, rec, st, p, call.shape, (const uint64_t*)d_entries,
+            launch_levels<uint64_t>(w, rec, st, p, call.shape, call.tune, (const uint64_t*)d_entries,
                 (uint32_t*)d_blob);
         }
         uint32_t status = 0;

@@ -1,0 +1,144 @@
+# SPDX-License-Identifier: Apache-2.0
+"""Per-size-class autotuner for the launch choices of the encoder.
+
+For each size class (log2 of the entry count) it times device-resident
+compresses of a seeded uniform permutation on the current GPU while forcing
+one setting at a time (bpb200_set_tuning), walking the knobs one after
+another (coordinate descent from the compiled defaults):
+
+  walk_blocks_per_sm  persistent orbit-walk blocks per SM
+  walk_max_log2       largest node coloured by orbit walks (else union-find)
+  jump_block_log2     largest super-ruler count jumped inside one CTA
+  tile_max_log2       largest node encoded by the shared-memory tile
+
+None of them may change a byte: every setting's blob is hashed and the run
+fails unless all hashes of a class agree.  The winners go to tuning.json
+beside the library, which the library reads at load; the per-class timings
+of the defaults and of the table go to the same file ("measured") and, with
+--summary, to a markdown table.
+
+Usage: python -m benes_perm_b200.tune [--classes 14,16,...] [--reps 5]
+           [--out benes_perm_b200/tuning.json] [--summary FILE]
+"""
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import statistics
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+CANDIDATES = {
+    "walk_blocks_per_sm": [2, 3, 4, 6],
+    "walk_max_log2": [16, 18, 20, 22, 23],
+    "jump_block_log2": [10, 12, 14, 16],
+    "tile_max_log2": [11, 12, 13],
+}
+
+
+def _workload(bp, log2n):
+    """The class's permutation: uniform, uint64 with the headline format at
+    2^27 entries and above, uint32 with the default format below."""
+    n = 1 << log2n
+    if log2n >= 27:
+        fmt = bp.FormatOptions(middle_group_log2=5,
+                               middle_placement=bp.MiddlePlacement.embedded_output)
+        dtype = np.uint64
+    else:
+        fmt = bp.FormatOptions()
+        dtype = np.uint32
+    return n, fmt, bp.fill_permutation(bp.PermutationKind.uniform, 0x7E5E + log2n, n, dtype)
+
+
+def tune_class(bp, torch, log2n, reps):
+    n, fmt, perm = _workload(bp, log2n)
+    width = perm.dtype.itemsize
+    size = bp.encoded_size(n, fmt)
+    d_in = torch.from_numpy(perm.view(np.int64 if width == 8 else np.int32)).cuda()
+    d_blob = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    hashes = set()
+
+    def measure(setting):
+        bp.set_tuning(setting)
+        try:
+            bp.compress_device(d_in.data_ptr(), n, width, d_blob.data_ptr(), size, fmt, stream)
+            times = [bp.compress_device(d_in.data_ptr(), n, width, d_blob.data_ptr(), size, fmt,
+                                        stream) for _ in range(reps)]
+        finally:
+            bp.set_tuning(None)
+        torch.cuda.synchronize()
+        hashes.add(hashlib.sha256(d_blob[:size].cpu().numpy().tobytes()).hexdigest())
+        return statistics.median(times)
+
+    bp.set_tuning(None)
+    defaults = bp.get_tuning(n)
+    # the compiled defaults, not whatever table is loaded now
+    compiled = dict(defaults, walk_blocks_per_sm=4, walk_max_log2=23, jump_block_log2=14,
+                    tile_max_log2=13)
+    best = dict(compiled)
+    best_t = measure(best)
+    default_t = best_t
+    tried = 1
+    for knob, values in CANDIDATES.items():
+        for v in values:
+            if v == best[knob]:
+                continue
+            trial = dict(best, **{knob: v})
+            t = measure(trial)
+            tried += 1
+            if t < best_t * 0.99:            # keep a change only for a clear gain
+                best, best_t = trial, t
+    if len(hashes) != 1:
+        raise SystemExit(f"class {log2n}: settings changed the output bytes ({len(hashes)} "
+                         "distinct blobs)")
+    return best, {"entries": n, "entry_bytes": width, "default_ms": default_t * 1e3,
+                  "tuned_ms": best_t * 1e3, "settings_tried": tried,
+                  "bytes_identical_across_settings": True}
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--classes", default="14,16,18,20,22,24,26,28,30")
+    ap.add_argument("--reps", type=int, default=5)
+    ap.add_argument("--out", default=os.path.join(HERE, "tuning.json"))
+    ap.add_argument("--summary", default=None)
+    args = ap.parse_args(argv)
+    sys.path.insert(0, os.path.dirname(HERE))
+    import torch
+    import benes_perm_b200 as bp
+    if not bp.backend_available():
+        raise SystemExit("no B200 device visible")
+    classes, measured = {}, {}
+    for c in [int(x) for x in args.classes.split(",") if x]:
+        best, rec = tune_class(bp, torch, c, args.reps)
+        classes[str(c)] = best
+        measured[str(c)] = rec
+        print(f"class 2^{c}: {rec['default_ms']:.3f} ms -> {rec['tuned_ms']:.3f} ms  {best}",
+              flush=True)
+    doc = {"device": torch.cuda.get_device_name(0),
+           "note": "made by benes_perm_b200/tune.py; the library reads 'classes'",
+           "classes": classes, "measured": measured}
+    with open(args.out, "w") as f:
+        json.dump(doc, f, indent=1, sort_keys=True)
+        f.write("\n")
+    if args.summary:
+        with open(args.summary, "w") as f:
+            f.write("| class | entries | width | default ms | tuned ms | gain | setting |\n")
+            f.write("|---|---|---|---|---|---|---|\n")
+            for c, rec in measured.items():
+                s = classes[c]
+                f.write(f"| 2^{c} | {rec['entries']} | {rec['entry_bytes']} B | "
+                        f"{rec['default_ms']:.3f} | {rec['tuned_ms']:.3f} | "
+                        f"{rec['default_ms'] / rec['tuned_ms']:.3f}x | "
+                        f"walk blocks/SM {s['walk_blocks_per_sm']}, walk max 2^{s['walk_max_log2']}, "
+                        f"one-CTA jump 2^{s['jump_block_log2']}, tile 2^{s['tile_max_log2']} |\n")
+
+
+if __name__ == "__main__":
+    main()

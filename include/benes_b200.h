@@ -197,6 +197,26 @@ void bpb200_shutdown(void);
  * and the total number of kernel launches; it returns the number of kinds. */
 void bpb200_set_profiling(int enabled);
 
+/* Launch tuning per size class (no reference counterpart; the reference's
+ * CUDA backend has one fixed launch shape, src/cuda/benes_cuda.cu:16).  None
+ * of these changes a byte of output.  The library reads its table from
+ * tuning.json beside the shared object (made by benes_perm_b200/tune.py;
+ * BPB200_TUNING_FILE names another file, "none" disables it); a class of
+ * ceil(log2 count) the table lacks takes its nearest class. */
+typedef struct bpb200_tuning {
+    uint32_t walk_blocks_per_sm; /* persistent orbit-walk blocks per SM, 1..8 */
+    uint32_t walk_max_log2;      /* largest node coloured by orbit walks (log2 entries) */
+    uint32_t jump_block_log2;    /* largest super-ruler count jumped inside one CTA (log2) */
+    uint32_t tile_max_log2;      /* largest node encoded by the shared-memory tile (log2), 9..13 */
+} bpb200_tuning;
+
+/* The setting calls with `count` entries use. */
+int bpb200_get_tuning(uint64_t count, bpb200_tuning* out);
+
+/* Tuner and test hook: a non-null setting is used by every later call
+ * (values clamped to their ranges); NULL returns to the table. */
+int bpb200_set_tuning(const bpb200_tuning* forced);
+
 /* Test hook: nonzero makes later calls colour every global level with the
  * union-find kernels instead of the orbit walks (the path the walks fall
  * back to on contrived inputs).  Output bytes are identical either way. */

@@ -37,6 +37,7 @@ enum BatchKind : int {
     kBJumpBlock,
     kBJump,
     kBCheck,
+    kBColour,
     kBUnion,
     kBOrient,
     kBFinalize,
@@ -230,6 +231,13 @@ __global__ void __launch_bounds__(32) batch_check(const LevelJob* jobs, uint32_t
     const LevelJob* j = level_job(jobs, n, kBCheck, &g);
     if (g.bid >= g.nblk || round > j->rounds || threadIdx.x != 0) return;
     ruler_check_run(g, round, j->control);
+}
+
+__global__ void __launch_bounds__(256) batch_colour(const LevelJob* jobs, uint32_t n) {
+    Grid g;
+    const LevelJob* j = level_job(jobs, n, kBColour, &g);
+    if (g.bid >= g.nblk) return;
+    ruler_colour_run(g, j->buckets, j->super_of, j->sstate, j->sstate + j->supers, j->control);
 }
 
 __global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) batch_union(const LevelJob* jobs,

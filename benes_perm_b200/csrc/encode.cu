@@ -576,15 +576,17 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
             if (one_block) {
                 ruler_jump_block<<<1, kJumpBlockThreads, 0, st>>>(sstate[0], sstate[1], supers,
                     rounds, ctl);
-                return;
+            } else {
+                const int gj = grid_for(supers, kLevelThreads);
+                for (uint32_t r = 0; r <= rounds; ++r) {
+                    ruler_jump<<<gj, kLevelThreads, 0, st>>>(sstate[r & 1], sstate[(r + 1) & 1],
+                        supers, r, ctl);
+                    ruler_check<<<1, 1, 0, st>>>(r, ctl);
+                }
             }
-            const int gj = grid_for(supers, kLevelThreads);
-            for (uint32_t r = 0; r <= rounds; ++r) {
-                ruler_jump<<<gj, kLevelThreads, 0, st>>>(sstate[r & 1], sstate[(r + 1) & 1],
-                    supers, r, ctl);
-                ruler_check<<<1, 1, 0, st>>>(r, ctl);
-            }
-        }, one_block ? 3 : 2 + 2 * (rounds + 1));
+            ruler_colour<<<gw, kLevelThreads, 0, st>>>(buckets, w.super_of, sstate[0], sstate[1],
+                ctl);
+        }, one_block ? 4 : 3 + 2 * (rounds + 1));
     }
     rec.launch(kKindUnion, [&] {
         level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, inv, w.uf, ctl + kCtlHard,

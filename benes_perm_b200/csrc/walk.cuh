@@ -571,6 +571,34 @@ __global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict
     ruler_super_short_run(launch_grid(), state, rulers, super_of, control);
 }
 
+// After the jumping: every ruler's colour, stamped into super_of in place
+// of its super-ruler (kColourTag | colour, the form ruler cycles without a
+// super-ruler already have), so level_finalize resolves a vertex's owner
+// with one dependent load instead of two.  The super-ruler states read here
+// are the buffer the last jumping round wrote (kCtlFinal).
+__device__ __forceinline__ void ruler_colour_run(Grid grid, uint32_t rulers,
+    uint32_t* __restrict__ super_of, const uint4* __restrict__ s0, const uint4* __restrict__ s1,
+    const uint32_t* control) {
+    if (*(volatile const uint32_t*)(control + kCtlHard) != 0) {
+        return; // the level is coloured by union-find
+    }
+    const uint4* state = control[kCtlFinal] ? s1 : s0;
+    for (uint32_t r = grid.bid * blockDim.x + threadIdx.x; r < rulers;
+         r += grid.nblk * blockDim.x) {
+        const uint32_t so = super_of[r];
+        if (so == kUnset || (so & kColourTag) != 0) {
+            continue;
+        }
+        const uint4 st = state[so >> kSuperLog2];
+        super_of[r] = kColourTag | (st.y > st.z ? 1u : 0u);
+    }
+}
+
+__global__ void __launch_bounds__(256) ruler_colour(uint32_t rulers, uint32_t* super_of,
+    const uint4* s0, const uint4* s1, const uint32_t* control) {
+    ruler_colour_run(launch_grid(), rulers, super_of, s0, s1, control);
+}
+
 // Clears the level's control words; `force_union_find` pre-sets the hard
 // flag so the level is coloured by union-find (a test hook for that path).
 __device__ __forceinline__ void control_reset_run(Grid grid, uint32_t* control, uint32_t force_union_find) {

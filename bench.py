@@ -217,6 +217,67 @@ def algorithmic_bytes(n, depth, tile, entry_bytes, switch_bits, middle_bits, wal
     return per, pipeline
 
 
+def random_accesses(n, tile, walk_levels, place_levels):
+    """Random 4-byte accesses per step by kernel kind and level, the least
+    each kind's algorithm needs (reads, writes): the inverse scatter one
+    write per entry (level 0 only; later inverses are written in order); a
+    union per output pair at least two finds and a link (a read per entry,
+    a write per pair); an orbit-walk step two gathers and an owner stamp
+    (two reads and a write per entry); finalize one lookup per pair-node
+    (find or owner-to-colour); the output pass one colour bit per output
+    pair."""
+    acc = {}
+    half = n / 2
+    for lvl in range(tile):
+        if lvl == 0:
+            acc[("place" if lvl in place_levels else "inverse", lvl)] = (0.0, float(n))
+        if lvl in walk_levels:
+            acc[("walk", lvl)] = (2.0 * n, float(n))
+        else:
+            acc[("union", lvl)] = (float(n), half)
+        acc[("resolve", lvl)] = (half, 0.0)
+        acc[("output_bits", lvl)] = (half, 0.0)
+    return acc
+
+
+def random_access_roofline(n, depth, tile, walk_levels, place_levels, node_log2, kernel_secs,
+                           probe):
+    """Per kernel kind: the time the least random accesses of its algorithm
+    take at the probed random-access rates, against the measured time.
+    Apart from the input and output streams every access of these kernels
+    is random, so this, not streaming bandwidth, is the bound that applies.
+    ``bound_l2_s`` takes every access at the L2-resident rates: a lower
+    bound on the time, hence ``frac`` <= 1.  ``bound_dram_s`` takes the DRAM
+    rates for levels whose nodes exceed 2^23 entries (their arrays do not
+    fit L2); a kind can beat it where its access order keeps them in L2
+    (claim-ordered work, the partitioned inverse)."""
+    bound_l2, bound_dram = {}, {}
+    l2, dram = probe["l2_32MB"], probe["dram_4GB"]
+    for (kind, lvl), (reads, writes) in random_accesses(n, tile, walk_levels,
+                                                         place_levels).items():
+        fast = reads / l2["reads_per_s"] + writes / l2["writes_per_s"]
+        rates = l2 if node_log2[lvl] <= 23 else dram
+        slow = reads / rates["reads_per_s"] + writes / rates["writes_per_s"]
+        bound_l2[kind] = bound_l2.get(kind, 0.0) + fast
+        bound_dram[kind] = bound_dram.get(kind, 0.0) + slow
+    kinds = {}
+    for kind, t in bound_l2.items():
+        measured = kernel_secs.get(kind, 0.0)
+        if measured > 0:
+            kinds[kind] = {"bound_l2_s": round(t, 6), "bound_dram_s": round(bound_dram[kind], 6),
+                           "measured_s": round(measured, 6), "frac": round(t / measured, 3)}
+    total_bound = sum(bound_l2.values())
+    total = sum(v for k, v in kernel_secs.items() if k in bound_l2)
+    return {"probe_accesses_per_s": {k: {kk: round(vv / 1e9, 1) for kk, vv in v.items()}
+                                     for k, v in probe.items()},
+            "probe_unit": "G accesses/s (4-byte; reads, writes, dependent chain steps)",
+            "kinds": kinds, "bound_l2_s": round(total_bound, 6),
+            "bound_dram_s": round(sum(bound_dram.values()), 6), "measured_s": round(total, 6),
+            "frac": round(total_bound / total, 3) if total else None,
+            "note": "least random 4-byte accesses of each kind's algorithm at the probed rates; "
+                    "the tile kernel (shared memory) is not included"}
+
+
 def measured_traffic(kind, n, node_log2s):
     """DRAM bytes per step of `kind` from the committed ncu summary
     (profiles/dram_traffic.json): bytes per entry of each level, measured
@@ -377,6 +438,9 @@ def b200_arm(args, world, rank, local):
         return bp.compress_device(d_in.data_ptr(), n, 8, d_blob.data_ptr(), size, fmt,
                                   stream.cuda_stream)
 
+    # random-access rates of this GPU (L2-resident and DRAM arrays), the
+    # bound of the encoder's kernels; measured before the timed steps
+    probe = {"l2_32MB": bp.probe_random_access(23), "dram_4GB": bp.probe_random_access(30)}
     for _ in range(max(args.warmup, 3)):
         step()
     _, _, launches_per_step = bp.last_profile()
@@ -398,6 +462,7 @@ def b200_arm(args, world, rank, local):
     kernel_counts = {}
     walk_levels = set()
     place_levels = set()
+    level_ms = {}
     with ClockSampler(gpu_index) as clocks:
         start.record(stream)
         for _ in range(args.steps):
@@ -409,6 +474,9 @@ def b200_arm(args, world, rank, local):
             marks = bp.last_profile_launches()
             walk_levels |= {lvl for kind, lvl, _ in marks if kind == "walk"}
             place_levels |= {lvl for kind, lvl, _ in marks if kind == "place"}
+            for kind, lvl, sec in marks:
+                row = level_ms.setdefault(lvl, {})
+                row[kind] = row.get(kind, 0.0) + sec * 1e3 / args.steps
         stop.record(stream)
         torch.cuda.synchronize()
     bp.set_profiling(False)
@@ -479,6 +547,8 @@ def b200_arm(args, world, rank, local):
         "achieved": pipeline_bytes / (secs / args.steps) / 1e9, "peak": peak, "unit": "GB/s",
         "frac": pipeline_bytes / (secs / args.steps) / 1e9 / peak,
     }
+    random_roof = random_access_roofline(n, depth, tile, walk_levels, place_levels, node_log2,
+                                         kernel_secs, probe)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": secs / args.steps * 1e3,
@@ -490,6 +560,9 @@ def b200_arm(args, world, rank, local):
         "gpu_launches": launches_per_step * args.steps,
         "roofline": roofline,
         "pipeline_roofline": pipeline,
+        "random_access_roofline": random_roof,
+        "per_level_ms": {str(l): {k: round(v, 3) for k, v in sorted(row.items())}
+                         for l, row in sorted(level_ms.items())},
         "kernel_seconds": {k: round(v, 6) for k, v in kernel_secs.items()},
         "kernel_launches": kernel_counts,
         "levels": {"depth": depth, "tile_level": tile, "walk_levels": sorted(walk_levels)},

@@ -348,6 +348,19 @@ def set_tuning(setting: Optional[dict]) -> None:
     lib.bpb200_set_tuning(ctypes.byref(t))
 
 
+def probe_random_access(log2_words: int) -> dict:
+    """Random 4-byte access rates (per second) of the GPU over an array of
+    2^log2_words words: reads, writes and dependent chain steps."""
+    lib = library()
+    d = ctypes.c_double
+    lib.bpb200_probe_random_access.argtypes = [ctypes.c_uint32, ctypes.POINTER(d),
+                                               ctypes.POINTER(d), ctypes.POINTER(d)]
+    r, w, c = d(0), d(0), d(0)
+    raise_for(lib.bpb200_probe_random_access(log2_words, ctypes.byref(r), ctypes.byref(w),
+                                             ctypes.byref(c)), "random-access probe failed")
+    return {"reads_per_s": r.value, "writes_per_s": w.value, "chain_steps_per_s": c.value}
+
+
 def describe(count: int, fmt: Optional[FormatOptions] = None):
     """(routing depth, first tile level) of the encode for (count, fmt)."""
     cf = to_c_format(fmt)

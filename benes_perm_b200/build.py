@@ -19,7 +19,7 @@ LIB = os.path.join(HERE, "libbenes_b200.so")
 SOURCES = ["encode.cu", "layout.cpp", "permgen.cpp"]
 HEADERS = ["plan.hpp", "layout.hpp", "device.cuh", "kernels.cuh", "tile.cuh", "walk.cuh",
            "batch_levels.cuh", "group.inc", "serve.inc", "file.inc", "staging.inc", "lookup.hpp",
-           "lookup.inc"]
+           "lookup.inc", "probe.inc"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -1329,3 +1329,6 @@ extern "C" int bpb200_compress_device_noalloc(const void* d_entries, uint64_t co
 
 // Batch lookup verifier (device twin of the reference's lookup).
 #include "lookup.inc"
+
+// Random-access roofline probe.
+#include "probe.inc"

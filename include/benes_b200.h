@@ -259,6 +259,15 @@ int bpb200_lookup_device(const void* d_blob, uint64_t blob_len, uint64_t count,
     const bpb200_format* format, const uint64_t* d_queries, uint64_t query_count, int inverse,
     uint64_t* d_out, void* stream, char* err, size_t err_len);
 
+/* Roofline probe (no reference counterpart): random 4-byte access rates
+ * of the current GPU over an array of 2^log2_words words (10..31; resident
+ * in L2 or not): independent random reads, independent random writes and
+ * dependent read chains, in accesses per second.  Allocates and frees its
+ * own buffer.  The encoder's kernels are bound by such accesses, so these
+ * rates, not the streaming copy bandwidth, bound them. */
+int bpb200_probe_random_access(uint32_t log2_words, double* reads_per_s,
+    double* writes_per_s, double* chain_steps_per_s);
+
 /* Host evaluation of the verifier's per-query walk (test hook, no device
  * work): one forward or inverse lookup in a host blob. */
 int bpb200_probe_lookup(uint64_t count, const bpb200_format* format, const uint8_t* blob,

@@ -112,7 +112,8 @@ def test_partitioned_inverse_levels(gpu, oracle):
     # Nodes above 2^23 entries (the walk limit) take the partitioned inverse
     # (level_bucket + level_place, profile kind "place") and union-find
     # colouring (no "walk" launch on that level); smaller global nodes take
-    # the plain inverse and the orbit walks.  n = 2^23 + 4097 puts level 0
+    # the orbit walks, with the inverse written by the parent's output pass
+    # (no inverse launch at all below level 0).  n = 2^23 + 4097 puts level 0
     # above the limit and level 1 below it.
     n = (1 << 23) + 4097
     kw = dict(middle_group_log2=4, middle_placement=2)
@@ -127,7 +128,7 @@ def test_partitioned_inverse_levels(gpu, oracle):
             walk = {lvl for k, lvl, _ in launches if k == "walk"}
             plain = {lvl for k, lvl, _ in launches if k == "inverse"}
             assert place == {0} and 0 not in walk and 0 not in plain, (kind, launches[:8])
-            assert 1 in walk and 1 in plain and 1 not in place
+            assert 1 in walk and not plain and 1 not in place
             assert got == oracle.compress(perm, oracle_format(kw)), (kind, dtype)
     finally:
         gpu.set_profiling(False)

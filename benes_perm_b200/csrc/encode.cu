@@ -237,8 +237,10 @@ TileShape tile_shape(const Plan& p, uint32_t t0) {
     TileShape s;
     s.slots = (uint32_t)std::min<uint64_t>(slots, 1u << 30);
     s.pairs = (uint32_t)std::min<uint64_t>(pairs, 1u << 30);
-    uint32_t off[9];
-    s.smem = tile_smem_layout(s.slots, s.pairs, off);
+    uint32_t off[10];
+    const uint32_t depth_below = p.depth - t0;
+    s.smem = depth_below < 24 ? tile_smem_layout(s.slots, s.pairs, 1u << depth_below, off)
+                              : UINT32_MAX;
     if (slots >= 65536 || pairs >= (1u << 30)) {
         s.smem = UINT32_MAX;
     }
@@ -604,8 +606,11 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
         // the next level's walk owners start unset and its pair-nodes as
         // roots; the tile level keeps its own state in shared memory
         const bool global_child = child_inv != nullptr;
+        // owners only matter where the orbit walks run
+        const bool child_walks = global_child && p.levels[l + 1].cap <= (1ull << tune.walk_max_log2)
+            && g_force_union_find.load() == 0;
         level_outputs<<<gp, kLevelThreads, 0, st>>>(dp, l, inv, w.xbits, w.ybits, child_inv,
-            global_child ? w.owner : nullptr, global_child ? w.uf : nullptr);
+            child_walks ? w.owner : nullptr, global_child ? w.uf : nullptr);
     });
     for (int side = 0; side < 2; ++side) {
         const uint32_t* bits = side == 0 ? w.xbits : w.ybits;

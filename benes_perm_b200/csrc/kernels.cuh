@@ -36,7 +36,8 @@
 
 namespace bpb200 {
 
-constexpr uint32_t kNodeWave = 256;   // node descriptors held in shared memory at once
+constexpr uint32_t kNodeWaveLog2 = 6;
+constexpr uint32_t kNodeWave = 1u << kNodeWaveLog2; // tile node descriptors held in shared memory at once
 constexpr uint32_t kTileThreads = 512;
 // 4 slots per thread measured fastest on B200 at 2^30 uniform entries
 // (inverse kernels 207 ms per compress; 8: 227 ms; 16: 243 ms): more

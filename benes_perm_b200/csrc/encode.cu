@@ -32,7 +32,9 @@ namespace bpb200 {
 namespace {
 
 constexpr uint64_t kTileMaxEntries = 8192;
-constexpr uint32_t kTileSmemBudget = 200 * 1024;
+constexpr uint32_t kTileSmemBudget = 224 * 1024;
+// Above this a tile runs as one 1024-thread CTA per SM (tile_encode_wide).
+constexpr uint32_t kTileSmemTwoPerSm = 112 * 1024;
 constexpr int kLevelThreads = 256;
 
 // Kernel kinds reported by bpb200_last_profile.
@@ -312,7 +314,7 @@ Tuning clamp_tuning(Tuning t) {
     t.walk_blocks_per_sm = clamp(t.walk_blocks_per_sm, 1, 8);
     t.walk_max_log2 = clamp(t.walk_max_log2, 10, BPB200_WALK_MAX_LOG2);
     t.jump_block_log2 = clamp(t.jump_block_log2, 4, 18);
-    t.tile_max_log2 = clamp(t.tile_max_log2, 9, 13);
+    t.tile_max_log2 = clamp(t.tile_max_log2, 9, 14);
     return t;
 }
 
@@ -690,18 +692,26 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     if (tiles > 0x7fffffffull) {
         throw CudaFail{cudaErrorInvalidValue, "too many tiles"};
     }
+    const bool wide = shape.smem > kTileSmemTwoPerSm;
+    auto launch_tile = [&](auto kernel, const auto* src, unsigned threads) {
+        allow_tile_smem((const void*)kernel);
+        rec.launch(kKindTile, [&] {
+            kernel<<<(unsigned)tiles, threads, shape.smem, st>>>(dp, src, d_blob, w.d_status,
+                shape.slots, shape.pairs);
+        });
+    };
     if (t0 == 0) {
-        allow_tile_smem((const void*)tile_encode<T>);
-        rec.launch(kKindTile, [&] {
-            tile_encode<T><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, d_in, d_blob,
-                w.d_status, shape.slots, shape.pairs);
-        });
+        if (wide) {
+            launch_tile(tile_encode_wide<T>, d_in, 2 * kTileThreads);
+        } else {
+            launch_tile(tile_encode<T>, d_in, kTileThreads);
+        }
     } else {
-        allow_tile_smem((const void*)tile_encode<uint32_t>);
-        rec.launch(kKindTile, [&] {
-            tile_encode<uint32_t><<<(unsigned)tiles, kTileThreads, shape.smem, st>>>(dp, cur32,
-                d_blob, w.d_status, shape.slots, shape.pairs);
-        });
+        if (wide) {
+            launch_tile(tile_encode_wide<uint32_t>, cur32, 2 * kTileThreads);
+        } else {
+            launch_tile(tile_encode<uint32_t>, cur32, kTileThreads);
+        }
     }
     check(cudaGetLastError(), "tile kernel launch");
 }

@@ -466,6 +466,17 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
     tile_body<T>(plan, src, blob, status, slots, pairs, blockIdx.x, smem);
 }
 
+// Tiles too large for two CTAs per SM (nodes of 16384 entries, about 200 KB
+// of shared memory): one CTA of twice the threads per SM keeps the same
+// number of resident warps.
+template <typename T>
+__global__ void __launch_bounds__(2 * kTileThreads, 1) tile_encode_wide(
+    const Plan* __restrict__ plan, const T* __restrict__ src, uint32_t* __restrict__ blob,
+    uint32_t* status, uint32_t slots, uint32_t pairs) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    tile_body<T>(plan, src, blob, status, slots, pairs, blockIdx.x, smem);
+}
+
 // Tiles of many permutations in one launch (the batched and serving forms):
 // job k owns blocks [first_block, first_block + tiles); the launch's dynamic
 // shared memory covers the largest job.

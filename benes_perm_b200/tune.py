@@ -37,7 +37,7 @@ CANDIDATES = {
     "walk_blocks_per_sm": [2, 3, 4, 6],
     "walk_max_log2": [16, 18, 20, 22, 23],
     "jump_block_log2": [10, 12, 14, 16],
-    "tile_max_log2": [11, 12, 13],
+    "tile_max_log2": [11, 12, 13, 14],
 }
 
 

@@ -207,7 +207,7 @@ typedef struct bpb200_tuning {
     uint32_t walk_blocks_per_sm; /* persistent orbit-walk blocks per SM, 1..8 */
     uint32_t walk_max_log2;      /* largest node coloured by orbit walks (log2 entries) */
     uint32_t jump_block_log2;    /* largest super-ruler count jumped inside one CTA (log2) */
-    uint32_t tile_max_log2;      /* largest node encoded by the shared-memory tile (log2), 9..13 */
+    uint32_t tile_max_log2;      /* largest node encoded by the shared-memory tile (log2), 9..14 */
 } bpb200_tuning;
 
 /* The setting calls with `count` entries use. */

@@ -38,6 +38,7 @@ def test_table_is_read_with_nearest_class_and_clamping(tmp_path, b200):
     assert got[0] == want16 and got[1] == want16 and got[2] == want16  # 2^16, class 16, nearest
     clamped = {"walk_blocks_per_sm": 8, "walk_max_log2": 23, "jump_block_log2": 4,
                "tile_max_log2": 9}
+    assert got[3]["tile_max_log2"] == 9
     assert got[3] == clamped and got[4] == clamped
     off = _query(dict(os.environ, BPB200_TUNING_FILE="none"), [1 << 20])[0]
     assert off == {"walk_blocks_per_sm": 4, "walk_max_log2": 23, "jump_block_log2": 14,
@@ -59,7 +60,8 @@ def test_every_setting_gives_the_same_bytes(gpu, oracle):
                 {"walk_blocks_per_sm": 2, "walk_max_log2": 16, "jump_block_log2": 10,
                  "tile_max_log2": 11},
                 {"walk_blocks_per_sm": 6, "walk_max_log2": 23, "jump_block_log2": 16,
-                 "tile_max_log2": 12}]
+                 "tile_max_log2": 12},
+                {"tile_max_log2": 14}]
     cases = [(70001, np.uint32, 0), (1 << 18, np.uint64, 1), (3 * (1 << 19) + 5, np.uint32, 0)]
     for n, dtype, kind in cases:
         perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0x7A + n, n, dtype)
@@ -70,6 +72,28 @@ def test_every_setting_gives_the_same_bytes(gpu, oracle):
                 blobs.append(gpu.compress(perm))
             finally:
                 gpu.set_tuning(None)
-        assert blobs[0] == blobs[1] == blobs[2], n
+        assert blobs[0] == blobs[1] == blobs[2] == blobs[3], n
         if n <= 1 << 18:
             assert blobs[0] == oracle.compress(perm)
+
+
+@pytest.mark.gpu
+def test_wide_tiles_of_16384_entries(gpu, oracle):
+    """tile_max_log2 = 14 hands nodes of up to 16384 entries to the
+    shared-memory tile (one 1024-thread CTA per SM); bytes stay the
+    reference's, including a permutation that is a single such tile."""
+    try:
+        gpu.set_tuning({"tile_max_log2": 14})
+        assert gpu.describe(1 << 20)[1] == 6
+        for n, dtype, kind in ((16384, np.uint32, 0), (16383, np.uint64, 1), (1 << 17, np.uint32, 0),
+                               (100003, np.uint64, 1)):
+            perm = gpu.fill_permutation(gpu.PermutationKind(kind), 0x1D + n, n, dtype)
+            for kw in (dict(), dict(middle_group_log2=2, middle_placement=1)):
+                fmt = gpu.FormatOptions(middle_group_log2=kw.get("middle_group_log2", 5),
+                                        middle_placement=gpu.MiddlePlacement(
+                                            kw.get("middle_placement", 0)))
+                from helpers import oracle_format
+                assert gpu.compress(perm, gpu.CompressOptions(format=fmt)) == \
+                    oracle.compress(perm, oracle_format(kw)), (n, kw)
+    finally:
+        gpu.set_tuning(None)

@@ -17,8 +17,11 @@
 //
 // Orbits are long for random inputs, so one vertex in every bucket of
 // 2^kRulerLog2 slots (at a hashed position) is a ruler.  A ruler walks its
-// orbit up to the next ruler, stamping each vertex it passes with its id
-// and keeping the minimum key of the segment and of the segment's mirror.
+// orbit up to the next ruler, stamping each even vertex it passes with its
+// id and keeping the minimum key of the segment and of the segment's
+// mirror.  Only even vertices are stamped: the colour of pair-node k is
+// the colour of vertex 2k, and halving the stamps halves the walk's
+// random writes.
 // Pointer jumping over rulers (stopping after the first round that changes
 // nothing, which implies convergence on cycles) turns segment minima into
 // orbit minima.  No atomics, no shared roots: every step is two independent
@@ -198,7 +201,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
                 next = (base + w) >> kRulerLog2;
                 end = true;
             } else {
-                if (w < s) owner[base + w] = r;
+                if (w < s && (w & 1u) == 0) owner[base + w] = r;
                 ma = min(ma, nv.key(w));
                 mb = min(mb, nv.key(w ^ 1u));
                 cur = w;
@@ -222,13 +225,14 @@ __global__ void __launch_bounds__(256) level_walk(const Plan* __restrict__ plan,
     level_walk_run<T>(launch_grid(), plan, level, vals, inv, owner, state, control);
 }
 
-// Cycles no ruler reached (both orbits ruler-free): thread per pair-node
-// whose two vertices are unowned.  Only the walker starting at the smallest
-// even vertex of its orbit walks the orbit whole (the others stop at the
-// first smaller even vertex, about log L steps), then stamps the orbit's
-// colour on every real vertex of it.  Every even vertex of the cycle lies in
-// one of the two orbits, so every pair-node of the cycle gets a stamped
-// colour; the cost is O(L log L) per cycle.
+// Orbits no ruler reached: thread per pair-node whose even vertex is
+// neither a ruler nor stamped, i.e. lies in a ruler-free orbit (its
+// mirror orbit may have rulers; the walk folds the mirror's keys as it
+// goes, so it needs nothing from them).  Only the walker starting at the
+// smallest even vertex of its orbit walks the orbit whole (the others stop
+// at the first smaller even vertex, about log L steps), then stamps the
+// orbit's colour on every real vertex of it; the cost is O(L log L) per
+// orbit, and such orbits are short for all but contrived inputs.
 template <typename T>
 __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ vals, const uint32_t* __restrict__ inv,
@@ -248,9 +252,6 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
         const uint32_t base = j * cap;
         const uint32_t v = 2 * k;
         if (is_ruler_slot(base + v) || owner[base + v] != kUnset) {
-            continue;
-        }
-        if (v + 1 < s && (is_ruler_slot(base + v + 1) || owner[base + v + 1] != kUnset)) {
             continue;
         }
         const NodeView<T> nv{vals + base, inv + base, s, (s & 1u) != 0};

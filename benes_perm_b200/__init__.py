@@ -384,6 +384,65 @@ def compress_device(d_entries: int, count: int, entry_bytes: int, d_blob: int, b
     return secs.value
 
 
+def compress_device_shard(d_entries: int, count: int, entry_bytes: int, d_blob: int,
+                          blob_len: int, shard: int, shards: int,
+                          fmt: Optional[FormatOptions] = None, stream: int = 0) -> float:
+    """One shard of a subtree-sharded compress (bpb200_compress_device_shard):
+    the blob receives shard `shard`'s bits only; the byte-wise sum of all
+    `shards` shards' blobs is the whole blob.  Returns device seconds."""
+    lib = library()
+    fp = ctypes.POINTER(_Format)
+    lib.bpb200_compress_device_shard.argtypes = [
+        ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, fp, ctypes.c_void_p, ctypes.c_uint64,
+        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+        ctypes.c_char_p, ctypes.c_size_t]
+    cf = to_c_format(fmt)
+    err = ctypes.create_string_buffer(512)
+    secs = ctypes.c_double(0)
+    rc = lib.bpb200_compress_device_shard(d_entries, count, entry_bytes, ctypes.byref(cf), d_blob,
+                                          blob_len, shard, shards, stream, ctypes.byref(secs),
+                                          err, 512)
+    raise_for(rc, err.value.decode())
+    return secs.value
+
+
+def combine_shards(blob, group=None, dst: int = 0):
+    """Sums the shards' blobs (a uint8 tensor per rank, the same length on
+    every rank) into rank `dst` over torch.distributed.  Every bit of the
+    blob is set by at most one shard, so the byte-wise sum carries nothing
+    and equals the OR of the shards: `dst` ends up with the whole blob.
+    Works with the NCCL and the gloo backends."""
+    import torch.distributed as dist
+    dist.reduce(blob, dst=dst, op=dist.ReduceOp.SUM, group=group)
+    return blob
+
+
+def compress_sharded(permutation, options: Optional[CompressOptions] = None, group=None):
+    """Subtree-sharded compress of one host permutation over the ranks of a
+    torch.distributed process group (one GPU each, the current device of
+    every rank): each rank encodes its shard and the shards are combined on
+    rank 0, which returns the blob bytes; the other ranks return None.  The
+    world size must be a power of two."""
+    import numpy as _np
+    import torch
+    import torch.distributed as dist
+    options = options or CompressOptions()
+    arr = _np.ascontiguousarray(permutation)
+    if arr.dtype not in (_np.uint32, _np.uint64):
+        raise TypeError("permutation must be uint32 or uint64")
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    n = int(arr.size)
+    size = encoded_size(n, options.format)
+    width = arr.dtype.itemsize
+    d_in = torch.from_numpy(arr.view(_np.int64 if width == 8 else _np.int32)).cuda()
+    d_blob = torch.zeros((size + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    compress_device_shard(d_in.data_ptr(), n, width, d_blob.data_ptr(), size, rank, world,
+                          options.format, stream)
+    combine_shards(d_blob, group)
+    return d_blob[:size].cpu().numpy().tobytes() if rank == 0 else None
+
+
 class _Request(ctypes.Structure):
     _fields_ = [
         ("d_entries", ctypes.c_void_p),

@@ -196,14 +196,14 @@ __global__ void __launch_bounds__(256) batch_super_walk(const LevelJob* jobs, ui
     Grid g;
     const LevelJob* j = level_job(jobs, n, kBSuperWalk, &g);
     if (g.bid >= g.nblk) return;
-    ruler_super_walk_run(g, j->state, j->buckets, j->sstate, j->super_of, j->control);
+    ruler_super_walk_run(g, j->state, 0u, j->buckets, j->sstate, j->super_of, j->control);
 }
 
 __global__ void __launch_bounds__(256) batch_super_short(const LevelJob* jobs, uint32_t n) {
     Grid g;
     const LevelJob* j = level_job(jobs, n, kBSuperShort, &g);
     if (g.bid >= g.nblk) return;
-    ruler_super_short_run(g, j->state, j->buckets, j->super_of, j->control);
+    ruler_super_short_run(g, j->state, 0u, j->buckets, j->super_of, j->control);
 }
 
 __global__ void __launch_bounds__(kJumpBlockThreads, 1) batch_jump_block(const LevelJob* jobs,
@@ -211,7 +211,8 @@ __global__ void __launch_bounds__(kJumpBlockThreads, 1) batch_jump_block(const L
     Grid g;
     const LevelJob* j = level_job(jobs, n, kBJumpBlock, &g);
     if (g.bid >= g.nblk) return;
-    ruler_jump_block_run(g, j->sstate, j->sstate + j->supers, j->supers, j->rounds, j->control);
+    ruler_jump_block_run(g, j->sstate, j->sstate + j->supers, 0u, j->supers, j->rounds,
+        j->control);
 }
 
 __global__ void __launch_bounds__(256) batch_jump(const LevelJob* jobs, uint32_t n,
@@ -221,7 +222,7 @@ __global__ void __launch_bounds__(256) batch_jump(const LevelJob* jobs, uint32_t
     if (g.bid >= g.nblk || round > j->rounds) return;
     uint4* s0 = j->sstate;
     uint4* s1 = j->sstate + j->supers;
-    ruler_jump_run(g, (round & 1u) ? s1 : s0, (round & 1u) ? s0 : s1, j->supers, round,
+    ruler_jump_run(g, (round & 1u) ? s1 : s0, (round & 1u) ? s0 : s1, 0u, j->supers, round,
         j->control);
 }
 
@@ -237,7 +238,8 @@ __global__ void __launch_bounds__(256) batch_colour(const LevelJob* jobs, uint32
     Grid g;
     const LevelJob* j = level_job(jobs, n, kBColour, &g);
     if (g.bid >= g.nblk) return;
-    ruler_colour_run(g, j->buckets, j->super_of, j->sstate, j->sstate + j->supers, j->control);
+    ruler_colour_run(g, 0u, j->buckets, j->super_of, j->sstate, j->sstate + j->supers,
+        j->control);
 }
 
 __global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) batch_union(const LevelJob* jobs,

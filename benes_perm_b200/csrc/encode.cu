@@ -475,30 +475,33 @@ struct Recorder {
 // least 32 nodes, else gathered per word), and the tail packets bit by bit
 // (`full` is the number of full packets, the first packet of the per-bit
 // form).
+// The block forms assemble words across the nodes of a cluster root, so a
+// sharded level uses them only when its nodes hold whole roots.
 template <typename F>
 void emission_launches(const Plan& p, uint32_t l, int side, F&& f) {
     const LevelInfo& lv = p.levels[l];
     const LevelSide& ls = lv.side[side];
+    const NodeRange nr = level_nodes(p, l);
     const uint32_t span_log2 = p.groups[side][ls.group].depth - ls.rel - 1;
     const uint64_t packets = (lv.cap / 2 + (1ull << span_log2) - 1) >> span_log2;
     if (span_log2 >= 5) {
-        f((int)kEmitWords, 0ull, grid_for(packets << (l + span_log2 - 5), kLevelThreads));
+        f((int)kEmitWords, 0ull, grid_for(packets << (nr.shift + span_log2 - 5), kLevelThreads));
         return;
     }
     const uint64_t half_min = lv.q / 2;
-    const uint64_t full = half_min >= 1 ? (half_min - 1) >> span_log2 : 0;
     const uint32_t rel = ls.rel;
+    const uint64_t full = half_min >= 1 && nr.shift >= rel ? (half_min - 1) >> span_log2 : 0;
     const uint32_t per_word_log2 = std::min<uint32_t>(5 - span_log2, rel);
     if (full > 0 && rel >= 5) {
         const uint64_t windows = (full + (32 >> span_log2) - 1) >> (5 - span_log2);
-        const uint64_t threads = (windows << (l - 5)) * 32;
+        const uint64_t threads = (windows << (nr.shift - 5)) * 32;
         f((int)kEmitTranspose, full, grid_for(threads, kLevelThreads));
     } else if (full > 0) {
-        const uint64_t words = (full << (rel - per_word_log2)) << (l - rel);
+        const uint64_t words = (full << (rel - per_word_log2)) << (nr.shift - rel);
         f((int)kEmitBlocks, full, grid_for(words, kLevelThreads));
     }
     f((int)kEmitBits, full,
-        grid_for((packets - std::min(packets, full)) << (l + span_log2), kLevelThreads));
+        grid_for((packets - std::min(packets, full)) << (nr.shift + span_log2), kLevelThreads));
 }
 
 // One global routing level: inverse (level 0 only; every later level's
@@ -513,16 +516,22 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
     uint32_t* child_inv) {
     const Plan* dp = w.d_plan;
     const LevelInfo& lv = p.levels[l];
+    // the whole level's extent (array layout), and this call's share of it
     const uint64_t slots = lv.cap << l;
-    const uint64_t prs = lv.pcap << l;
-    const uint64_t nodes = 1ull << l;
     const uint32_t buckets = (uint32_t)((slots + (1u << kRulerLog2) - 1) >> kRulerLog2);
+    const NodeRange nr = level_nodes(p, l);
+    const RulerRange rr = ruler_range(p, l);
+    const uint32_t slo = (rr.lo + (1u << kSuperLog2) - 1) >> kSuperLog2;
+    const uint32_t shi = (rr.hi + (1u << kSuperLog2) - 1) >> kSuperLog2;
+    const uint64_t prs = lv.pcap << nr.shift;
+    const uint64_t nodes = 1ull << nr.shift;
+    const uint32_t my_buckets = rr.hi - rr.lo;
     const int gs = grid_for((slots + kInverseItems - 1) / kInverseItems, kLevelThreads);
     const int gu = grid_for((prs + kUnionItems - 1) / kUnionItems, kLevelThreads);
     const int gr = grid_for((prs + kResolveItems - 1) / kResolveItems, kLevelThreads);
     const int gp = grid_for(prs, kLevelThreads);
     const int gn = grid_for(nodes, kLevelThreads);
-    const int gw = grid_for(buckets, kLevelThreads);
+    const int gw = grid_for(my_buckets, kLevelThreads);
     uint32_t* ctl = w.control;
     // nodes whose arrays do not fit in L2 are coloured by union-find
     const bool walks = lv.cap <= (1ull << tune.walk_max_log2) && g_force_union_find.load() == 0;
@@ -553,7 +562,7 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
             int dev = 0, sms = 148;
             cudaGetDevice(&dev);
             cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-            const uint64_t want = ((uint64_t)buckets + kWalkChunk - 1) / kWalkChunk * 32;
+            const uint64_t want = ((uint64_t)my_buckets + kWalkChunk - 1) / kWalkChunk * 32;
             const int gwalk = (int)std::max<uint64_t>(1,
                 std::min<uint64_t>((uint64_t)sms * tune.walk_blocks_per_sm,
                     (want + kLevelThreads - 1) / kLevelThreads));
@@ -570,26 +579,27 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
         }
         uint4* sstate[2] = {w.state[1], w.state[1] + supers};
         // few super-rulers: every round in one CTA; otherwise one launch pair per round
-        const bool one_block = supers <= (1u << tune.jump_block_log2);
+        const bool one_block = shi - slo <= (1u << tune.jump_block_log2);
         rec.launch(kKindJump, [&] {
             check(cudaMemsetAsync(w.super_of, 0xff, (uint64_t)buckets * 4, st),
                 "cudaMemsetAsync(super rulers)");
-            ruler_super_walk<<<grid_for(supers, kLevelThreads), kLevelThreads, 0, st>>>(
-                w.state[0], buckets, sstate[0], w.super_of, ctl);
-            ruler_super_short<<<gw, kLevelThreads, 0, st>>>(w.state[0], buckets, w.super_of, ctl);
+            ruler_super_walk<<<grid_for(shi - slo, kLevelThreads), kLevelThreads, 0, st>>>(
+                w.state[0], rr.lo, rr.hi, sstate[0], w.super_of, ctl);
+            ruler_super_short<<<gw, kLevelThreads, 0, st>>>(w.state[0], rr.lo, rr.hi, w.super_of,
+                ctl);
             if (one_block) {
-                ruler_jump_block<<<1, kJumpBlockThreads, 0, st>>>(sstate[0], sstate[1], supers,
+                ruler_jump_block<<<1, kJumpBlockThreads, 0, st>>>(sstate[0], sstate[1], slo, shi,
                     rounds, ctl);
             } else {
-                const int gj = grid_for(supers, kLevelThreads);
+                const int gj = grid_for(shi - slo, kLevelThreads);
                 for (uint32_t r = 0; r <= rounds; ++r) {
                     ruler_jump<<<gj, kLevelThreads, 0, st>>>(sstate[r & 1], sstate[(r + 1) & 1],
-                        supers, r, ctl);
+                        slo, shi, r, ctl);
                     ruler_check<<<1, 1, 0, st>>>(r, ctl);
                 }
             }
-            ruler_colour<<<gw, kLevelThreads, 0, st>>>(buckets, w.super_of, sstate[0], sstate[1],
-                ctl);
+            ruler_colour<<<gw, kLevelThreads, 0, st>>>(rr.lo, rr.hi, w.super_of, sstate[0],
+                sstate[1], ctl);
         }, one_block ? 4 : 3 + 2 * (rounds + 1));
     }
     rec.launch(kKindUnion, [&] {
@@ -614,7 +624,10 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
         level_outputs<<<gp, kLevelThreads, 0, st>>>(dp, l, inv, w.xbits, w.ybits, child_inv,
             child_walks ? w.owner : nullptr, global_child ? w.uf : nullptr);
     });
-    for (int side = 0; side < 2; ++side) {
+    // above the shard level every shard computes the level, shard 0 alone
+    // writes its switches
+    const bool emit = p.shards <= 1 || l >= p.shard_level || p.shard == 0;
+    for (int side = 0; side < 2 && emit; ++side) {
         const uint32_t* bits = side == 0 ? w.xbits : w.ybits;
         emission_launches(p, l, side, [&](int form, uint64_t full, int blocks) {
             rec.launch(kKindEmit, [&] {
@@ -688,7 +701,7 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         cur32 = dst;
     }
     rec.level = (int)t0;
-    const uint64_t tiles = 1ull << t0;
+    const uint64_t tiles = 1ull << level_nodes(p, t0).shift;
     if (tiles > 0x7fffffffull) {
         throw CudaFail{cudaErrorInvalidValue, "too many tiles"};
     }
@@ -827,7 +840,8 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     check(cudaMemcpyAsync(w.d_plan, w.h_plan, sizeof(Plan), cudaMemcpyHostToDevice, st),
         "plan upload");
     Header h{};
-    h.bytes = (uint32_t)call.layout.header_bytes;
+    // of the shards of one permutation only shard 0 writes the header
+    h.bytes = p.shards > 1 && p.shard != 0 ? 0u : (uint32_t)call.layout.header_bytes;
     write_header(call.layout, h.data);
     check(cudaEventRecord(w.start, st), "cudaEventRecord");
     check(cudaMemsetAsync(d_blob, 0, (p.end_offset + 3) / 4 * 4, st), "cudaMemsetAsync(blob)");
@@ -1047,6 +1061,43 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
             return rc;
         }
         // the work is queued on the caller's stream, after its earlier work
+        return run(w, call, (cudaStream_t)stream, d_entries, entry_bytes, (uint32_t*)d_blob,
+            device_seconds, err, err_len);
+    });
+}
+
+int bpb200_compress_device_shard(const void* d_entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, uint32_t shard,
+    uint32_t shards, void* stream, double* device_seconds, char* err, size_t err_len) {
+    return guarded(err, err_len, [&]() -> int {
+        int device = 0;
+        if (!current_device_ok(&device)) {
+            set_error(err, err_len, "b200 backend is unavailable");
+            return kUnavailable;
+        }
+        if (shards == 0 || (shards & (shards - 1)) != 0 || shard >= shards) {
+            set_error(err, err_len, "shards must be a power of two and shard below it");
+            return kInvalidArgument;
+        }
+        if (const int bad = check_device_buffers(d_entries, entry_bytes, d_blob, err, err_len)) {
+            return bad;
+        }
+        Lease lease(device);
+        Workspace& w = *lease.w;
+        Call call;
+        int rc = prepare(count, entry_bytes, format, blob_len, w, &call, err, err_len);
+        if (rc != kOk) {
+            return rc;
+        }
+        uint32_t k = 0;
+        while ((1u << k) < shards) ++k;
+        if (k > call.plan->tile_level) {
+            set_error(err, err_len, "permutation too small for that many shards");
+            return kInvalidArgument;
+        }
+        call.plan->shards = shards;
+        call.plan->shard = shard;
+        call.plan->shard_level = k;
         return run(w, call, (cudaStream_t)stream, d_entries, entry_bytes, (uint32_t*)d_blob,
             device_seconds, err, err_len);
     });

@@ -307,11 +307,14 @@ __device__ __forceinline__ void level_union_run(Grid grid, const Plan* __restric
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
-    const uint64_t total = (uint64_t)pcap << level;
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t begin = nr.lo * pcap;
+    const uint64_t total = (uint64_t)pcap << nr.shift;
+    const uint64_t end = begin + total;
     uint64_t first;
     while (claim_chunk(claims, (uint64_t)blockDim.x * kUnionItems, total, &first)) {
-        const uint64_t p0 = first + (uint64_t)threadIdx.x * kUnionItems;
-        if (p0 >= total) {
+        const uint64_t p0 = begin + first + (uint64_t)threadIdx.x * kUnionItems;
+        if (p0 >= end) {
             continue;
         }
         uint32_t j = (uint32_t)(p0 / pcap);
@@ -322,7 +325,7 @@ __device__ __forceinline__ void level_union_run(Grid grid, const Plan* __restric
         uint32_t pending = 0;
 #pragma unroll
         for (int q = 0; q < kUnionItems; ++q) {
-            if (p0 + q < total && k < s / 2) {
+            if (p0 + q < end && k < s / 2) {
                 pending |= 1u << q;
                 const uint64_t at = (uint64_t)j * cap + 2 * k;
                 u[q] = inv[at];
@@ -367,8 +370,9 @@ __device__ __forceinline__ void level_orient_run(Grid grid, const Plan* __restri
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
-    const uint64_t nodes = 1ull << level;
-    for (uint64_t j = (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes;
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t nodes_end = nr.lo + (1ull << nr.shift);
+    for (uint64_t j = nr.lo + (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes_end;
          j += (uint64_t)grid.nblk * blockDim.x) {
         const uint32_t s = size_at(lv, level, (uint32_t)j);
         if ((s & 1u) == 0) {
@@ -392,8 +396,9 @@ __global__ void level_orient(const Plan* __restrict__ plan, uint32_t level,
 
 __device__ __forceinline__ void level_descriptors_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     NodeAddress* __restrict__ in_addr, NodeAddress* __restrict__ out_addr) {
-    const uint64_t nodes = 1ull << level;
-    for (uint64_t j = (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes;
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t nodes_end = nr.lo + (1ull << nr.shift);
+    for (uint64_t j = nr.lo + (uint64_t)grid.bid * blockDim.x + threadIdx.x; j < nodes_end;
          j += (uint64_t)grid.nblk * blockDim.x) {
         in_addr[j] = node_address(*plan, 0, level, j);
         out_addr[j] = node_address(*plan, 1, level, j);
@@ -433,12 +438,17 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint32_t ccap = (uint32_t)cl.cap;
     const uint32_t cpcap = (uint32_t)cl.pcap;
-    const uint64_t total = (uint64_t)pcap << level;
+    // this call's output pairs; the loop starts at a 32-pair boundary so
+    // each warp assembles whole bit words (bits before `first` stay zero)
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t first = nr.lo * pcap;
+    const uint64_t end = first + ((uint64_t)pcap << nr.shift);
+    const uint64_t begin = first & ~31ull;
     const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
-    for (uint64_t p = (uint64_t)grid.bid * blockDim.x + threadIdx.x;
-         p - (threadIdx.x & 31) < total; p += stride) {
+    for (uint64_t p = begin + (uint64_t)grid.bid * blockDim.x + threadIdx.x;
+         p - (threadIdx.x & 31) < end; p += stride) {
         bool y = false;
-        if (p < total) {
+        if (p >= first && p < end) {
             const uint32_t j = (uint32_t)(p / pcap);
             const uint32_t k = (uint32_t)(p - (uint64_t)j * pcap);
             const uint32_t s = size_at(lv, level, j);
@@ -510,7 +520,8 @@ __device__ __forceinline__ void level_emit_run(Grid grid, const Plan* __restrict
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t max_pairs = lv.cap / 2;
     const uint64_t packets = (max_pairs + (1ull << span_log2) - 1) >> span_log2;
-    const uint32_t shift = level + span_log2; // log2(nodes * span)
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint32_t shift = nr.shift + span_log2; // log2(nodes * span)
     const uint64_t total = packets > first_packet ? (packets - first_packet) << shift : 0;
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
@@ -521,7 +532,7 @@ __device__ __forceinline__ void level_emit_run(Grid grid, const Plan* __restrict
         if (t < total) {
             const uint64_t packet = first_packet + (t >> shift);
             const uint64_t rem = t & ((1ull << shift) - 1);
-            const uint32_t node = (uint32_t)(rem >> span_log2);
+            const uint32_t node = (uint32_t)(nr.lo + (rem >> span_log2));
             const uint64_t pair = (packet << span_log2) + (rem & ((1ull << span_log2) - 1));
             const uint32_t s = size_at(lv, level, node);
             if (pair < s / 2) {
@@ -564,12 +575,16 @@ __device__ __forceinline__ void level_emit_blocks_run(Grid grid, const Plan* __r
     const uint32_t per_word_log2 = min(5u - span_log2, rel);
     const uint32_t words_log2 = rel - per_word_log2; // words per block (log2)
     const uint64_t per_root = full_packets << words_log2;
-    const uint64_t total = (per_root << (level - rel));
+    // this call's nodes hold whole cluster roots (the host uses this form
+    // only then)
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t root_lo = nr.lo >> rel;
+    const uint64_t total = (per_root << (nr.shift - rel));
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
     for (uint64_t t = (uint64_t)grid.bid * blockDim.x + threadIdx.x; t < total; t += stride) {
-        const uint64_t root = t / per_root;
-        const uint64_t rem = t - root * per_root;
+        const uint64_t root = root_lo + t / per_root;
+        const uint64_t rem = t - (root - root_lo) * per_root;
         const uint64_t packet = rem >> words_log2;
         const uint32_t word = (uint32_t)(rem & ((1ull << words_log2) - 1));
         const uint32_t node0 = (uint32_t)(root << rel) + (word << per_word_log2);
@@ -619,7 +634,9 @@ __device__ __forceinline__ void level_emit_transpose_run(Grid grid, const Plan* 
     const uint32_t per_window_log2 = 5 - span_log2; // packets per lane window
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint64_t windows = (full_packets + (1ull << per_window_log2) - 1) >> per_window_log2;
-    const uint64_t groups = 1ull << (level - 5);  // 32-node groups over all roots
+    // 32-node groups of this call's nodes (at least 32 of them, aligned)
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t groups = 1ull << (nr.shift - 5);
     const uint64_t total_warps = groups * windows;
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint32_t lane = threadIdx.x & 31;
@@ -628,7 +645,7 @@ __device__ __forceinline__ void level_emit_transpose_run(Grid grid, const Plan* 
          wi += warps) {
         const uint64_t group = wi / windows;
         const uint64_t k0 = (wi - group * windows) << per_window_log2;
-        const uint32_t node = (uint32_t)(group << 5) + lane;
+        const uint32_t node = (uint32_t)(nr.lo + (group << 5)) + lane;
         const uint64_t q = (uint64_t)node * pcap + (k0 << span_log2);
         const uint64_t wq = q >> 5;
         uint32_t window = __funnelshift_r(bits[wq], bits[wq + 1], (uint32_t)(q & 31));
@@ -686,14 +703,15 @@ __device__ __forceinline__ void level_emit_words_run(Grid grid, const Plan* __re
     const uint64_t max_pairs = lv.cap / 2;
     const uint64_t packets = (max_pairs + (1ull << span_log2) - 1) >> span_log2;
     const uint32_t cshift = span_log2 - 5;  // log2(chunks per run)
-    const uint32_t shift = level + cshift;  // log2(nodes * chunks per run)
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint32_t shift = nr.shift + cshift; // log2(nodes * chunks per run)
     const uint64_t total = packets << shift;
     const uint64_t section_bit = plan->section_offset[side] * 8;
     const uint64_t stride = (uint64_t)grid.nblk * blockDim.x;
     for (uint64_t t = (uint64_t)grid.bid * blockDim.x + threadIdx.x; t < total; t += stride) {
         const uint64_t packet = t >> shift;
         const uint64_t rem = t & ((1ull << shift) - 1);
-        const uint32_t node = (uint32_t)(rem >> cshift);
+        const uint32_t node = (uint32_t)(nr.lo + (rem >> cshift));
         const uint64_t pair0 = (packet << span_log2) + ((rem & ((1ull << cshift) - 1)) << 5);
         const uint64_t half = size_at(lv, level, node) / 2;
         if (pair0 >= half) {

@@ -76,10 +76,32 @@ struct Plan {
     uint64_t max_slots;         // max over levels of 2^l * cap_l
     uint64_t max_pairs;         // max over levels of 2^l * pcap_l
     uint32_t fact_bits[33];     // ceil(log2(c!)) for c = 0..32
-    uint32_t pad2_;
+    // Subtree sharding: with shards = 2^shard_level > 1 this call encodes
+    // every node of the levels above shard_level and, from shard_level on,
+    // only the subtree of node `shard` of level shard_level (see
+    // level_nodes).  0 or 1: the whole permutation.
+    uint32_t shards;
+    uint32_t shard;
+    uint32_t shard_level;
     GroupInfo groups[2][kMaxGroups];
     LevelInfo levels[kMaxLevels + 1];
 };
+
+// The nodes of `level` this call encodes: [lo, lo + 2^shift).  Without
+// sharding, and above the shard level, every node of the level; from the
+// shard level on, the 2^(level - shard_level) descendants of node `shard`
+// of the shard level, which are consecutive and aligned.
+struct NodeRange {
+    uint64_t lo;
+    uint32_t shift;
+};
+
+BP_HD NodeRange level_nodes(const Plan& p, uint32_t level) {
+    if (p.shards <= 1 || level < p.shard_level) {
+        return NodeRange{0, level};
+    }
+    return NodeRange{(uint64_t)p.shard << (level - p.shard_level), level - p.shard_level};
+}
 
 // ---------------------------------------------------------------- bit math
 

@@ -463,7 +463,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
     uint32_t pairs) {
     extern __shared__ __align__(16) unsigned char smem[];
-    tile_body<T>(plan, src, blob, status, slots, pairs, blockIdx.x, smem);
+    // a sharded call encodes only its own tiles (level_nodes)
+    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo;
+    tile_body<T>(plan, src, blob, status, slots, pairs, first + blockIdx.x, smem);
 }
 
 // Tiles too large for two CTAs per SM (nodes of 16384 entries, about 200 KB
@@ -474,7 +476,8 @@ __global__ void __launch_bounds__(2 * kTileThreads, 1) tile_encode_wide(
     const Plan* __restrict__ plan, const T* __restrict__ src, uint32_t* __restrict__ blob,
     uint32_t* status, uint32_t slots, uint32_t pairs) {
     extern __shared__ __align__(16) unsigned char smem[];
-    tile_body<T>(plan, src, blob, status, slots, pairs, blockIdx.x, smem);
+    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo;
+    tile_body<T>(plan, src, blob, status, slots, pairs, first + blockIdx.x, smem);
 }
 
 // Tiles of many permutations in one launch (the batched and serving forms):

@@ -96,6 +96,23 @@ __device__ __forceinline__ bool is_ruler_slot(uint32_t slot) {
     return (slot & ((1u << kRulerLog2) - 1)) == ruler_position(slot >> kRulerLog2);
 }
 
+// The rulers of this call's nodes (level_nodes): buckets [lo, hi) covering
+// slots [slot_lo, slot_end).  A bucket at either end may hash its ruler
+// into a neighbouring node outside the range; such rulers are marked absent.
+struct RulerRange {
+    uint32_t lo, hi;
+    uint64_t slot_lo, slot_end;
+};
+
+BP_HD RulerRange ruler_range(const Plan& p, uint32_t level) {
+    const LevelInfo& lv = p.levels[level];
+    const NodeRange nr = level_nodes(p, level);
+    const uint64_t slot_lo = nr.lo * lv.cap;
+    const uint64_t slot_end = slot_lo + (lv.cap << nr.shift);
+    return RulerRange{(uint32_t)(slot_lo >> kRulerLog2),
+        (uint32_t)((slot_end + (1u << kRulerLog2) - 1) >> kRulerLog2), slot_lo, slot_end};
+}
+
 // One node of one level, as seen by a walker.
 template <typename T>
 struct NodeView {
@@ -139,8 +156,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
     uint4* __restrict__ state, uint32_t* control) {
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
-    const uint64_t total = (uint64_t)cap << level;
-    const uint32_t buckets = (uint32_t)((total + (1u << kRulerLog2) - 1) >> kRulerLog2);
+    const RulerRange rr = ruler_range(*plan, level);
     const uint32_t lane = threadIdx.x & 31;
     const unsigned below = (1u << lane) - 1u;
     uint32_t next_free = 0, hi = 0; // current chunk, warp-uniform
@@ -154,12 +170,12 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
             uint32_t c = 0;
             if (lane == 0) c = atomicAdd(control + kCtlClaim, 1u);
             c = __shfl_sync(0xffffffffu, c, 0);
-            const uint64_t lo = (uint64_t)c * kWalkChunk;
-            if (lo >= buckets) {
+            const uint64_t lo = rr.lo + (uint64_t)c * kWalkChunk;
+            if (lo >= rr.hi) {
                 exhausted = true;
             } else {
                 next_free = (uint32_t)lo;
-                hi = (uint32_t)(lo + kWalkChunk < buckets ? lo + kWalkChunk : buckets);
+                hi = (uint32_t)(lo + kWalkChunk < rr.hi ? lo + kWalkChunk : rr.hi);
             }
         }
         if (!active) {
@@ -167,10 +183,11 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
             if (mine < hi) {
                 r = mine;
                 const uint32_t slot = (r << kRulerLog2) + ruler_position(r);
-                const uint32_t j = slot < total ? slot / cap : 0u;
+                const bool in_range = slot >= rr.slot_lo && slot < rr.slot_end;
+                const uint32_t j = in_range ? slot / cap : 0u;
                 const uint32_t v0 = slot - j * cap;
-                s = slot < total ? size_at(lv, level, j) : 0u;
-                if (slot >= total || v0 >= s) {
+                s = in_range ? size_at(lv, level, j) : 0u;
+                if (!in_range || v0 >= s) {
                     state[r] = make_uint4(kNoRuler, 0, 0, 0);
                 } else {
                     base = j * cap;
@@ -240,8 +257,9 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
-    const uint64_t total = (uint64_t)pcap << level;
-    for (uint64_t pidx = (uint64_t)grid.bid * blockDim.x + threadIdx.x; pidx < total;
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t end = (nr.lo + (1ull << nr.shift)) * pcap;
+    for (uint64_t pidx = nr.lo * pcap + (uint64_t)grid.bid * blockDim.x + threadIdx.x; pidx < end;
          pidx += (uint64_t)grid.nblk * blockDim.x) {
         const uint32_t j = (uint32_t)(pidx / pcap);
         const uint32_t k = (uint32_t)(pidx - (uint64_t)j * pcap);
@@ -305,8 +323,11 @@ __global__ void __launch_bounds__(256) level_walk_short(const Plan* __restrict__
 // (and, early on, the near successors they read) stay close together.
 // The done/hard words were written by earlier launches, so every thread of
 // a block sees the same value and the block leaves together.
+// States [lo, hi) are this call's super-rulers (all of them unless the
+// level is sharded); a successor outside them can only come from a
+// non-permutation and sends the level to union-find.
 __device__ __forceinline__ void ruler_jump_run(Grid grid, const uint4* __restrict__ src,
-    uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
+    uint4* __restrict__ dst, uint32_t lo, uint32_t hi, uint32_t round, uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
         *(volatile uint32_t*)(control + kCtlHard) != 0) {
         return;
@@ -314,14 +335,16 @@ __device__ __forceinline__ void ruler_jump_run(Grid grid, const uint4* __restric
     bool changed = false;
     const uint64_t chunk = (uint64_t)blockDim.x * kJumpItems;
     uint64_t first = 0;
-    while (claim_chunk(control + kCtlClaimJump, chunk, rulers, &first)) {
+    bool bad = false;
+    while (claim_chunk(control + kCtlClaimJump, chunk, hi - lo, &first)) {
         for (uint32_t k = 0; k < kJumpItems; ++k) {
-            const uint64_t r = first + (uint64_t)k * blockDim.x + threadIdx.x;
-            if (r >= rulers) {
+            const uint64_t r = lo + first + (uint64_t)k * blockDim.x + threadIdx.x;
+            if (r >= hi) {
                 break;
             }
             const uint4 me = src[r];
-            if (me.x == kNoRuler) {
+            if (me.x == kNoRuler || me.x < lo || me.x >= hi) {
+                bad |= me.x != kNoRuler;
                 dst[r] = me;
                 continue;
             }
@@ -334,12 +357,15 @@ __device__ __forceinline__ void ruler_jump_run(Grid grid, const uint4* __restric
     if (__any_sync(0xffffffffu, changed) && (threadIdx.x & 31) == 0) {
         atomicOr(control + kCtlChanged, 1u);
     }
+    if (bad) {
+        atomicOr(control + kCtlHard, 1u);
+    }
     (void)round;
 }
 
 __global__ void __launch_bounds__(256) ruler_jump(const uint4* __restrict__ src,
-    uint4* __restrict__ dst, uint32_t rulers, uint32_t round, uint32_t* control) {
-    ruler_jump_run(launch_grid(), src, dst, rulers, round, control);
+    uint4* __restrict__ dst, uint32_t lo, uint32_t hi, uint32_t round, uint32_t* control) {
+    ruler_jump_run(launch_grid(), src, dst, lo, hi, round, control);
 }
 
 // After a round: a round that changed nothing means every ruler holds its
@@ -376,7 +402,7 @@ constexpr uint32_t kJumpBlockBatch = 4;
 constexpr uint32_t kJumpBlockMaxStates = 1u << BPB200_JUMP_BLOCK_LOG2;
 
 __device__ __forceinline__ void ruler_jump_block_run(Grid grid, uint4* s0, uint4* s1,
-    uint32_t supers, uint32_t rounds, uint32_t* control) {
+    uint32_t lo, uint32_t hi, uint32_t rounds, uint32_t* control) {
     // written by earlier launches: every thread reads the same values
     if (*(volatile uint32_t*)(control + kCtlDone) != 0 ||
         *(volatile uint32_t*)(control + kCtlHard) != 0) {
@@ -395,26 +421,27 @@ __device__ __forceinline__ void ruler_jump_block_run(Grid grid, uint4* s0, uint4
         const uint4* src = (r & 1u) ? s1 : s0;
         uint4* dst = (r & 1u) ? s0 : s1;
         bool ch = false;
-        for (uint32_t base = 0; base < supers; base += kJumpBlockThreads * kJumpBlockBatch) {
+        for (uint32_t base = lo; base < hi; base += kJumpBlockThreads * kJumpBlockBatch) {
             uint4 me[kJumpBlockBatch], nx[kJumpBlockBatch];
 #pragma unroll
             for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
                 const uint32_t i = base + k * kJumpBlockThreads + threadIdx.x;
-                me[k] = i < supers ? __ldcg(src + i) : make_uint4(kNoRuler, 0u, 0u, 0u);
+                me[k] = i < hi ? __ldcg(src + i) : make_uint4(kNoRuler, 0u, 0u, 0u);
             }
 #pragma unroll
             for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
-                const bool live = me[k].x != kNoRuler && me[k].x < supers;
-                bad |= me[k].x != kNoRuler && me[k].x >= supers;
+                const bool inside = me[k].x >= lo && me[k].x < hi;
+                const bool live = me[k].x != kNoRuler && inside;
+                bad |= me[k].x != kNoRuler && !inside;
                 nx[k] = live ? __ldcg(src + me[k].x) : me[k];
             }
 #pragma unroll
             for (uint32_t k = 0; k < kJumpBlockBatch; ++k) {
                 const uint32_t i = base + k * kJumpBlockThreads + threadIdx.x;
-                if (i >= supers) {
+                if (i >= hi) {
                     continue;
                 }
-                if (me[k].x == kNoRuler || me[k].x >= supers) {
+                if (me[k].x == kNoRuler || me[k].x < lo || me[k].x >= hi) {
                     dst[i] = me[k];
                     continue;
                 }
@@ -453,8 +480,8 @@ __device__ __forceinline__ void ruler_jump_block_run(Grid grid, uint4* s0, uint4
 }
 
 __global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* s0, uint4* s1,
-    uint32_t supers, uint32_t rounds, uint32_t* control) {
-    ruler_jump_block_run(launch_grid(), s0, s1, supers, rounds, control);
+    uint32_t lo, uint32_t hi, uint32_t rounds, uint32_t* control) {
+    ruler_jump_block_run(launch_grid(), s0, s1, lo, hi, rounds, control);
 }
 
 // ---------------------------------------------------------------------------
@@ -469,17 +496,20 @@ __global__ void __launch_bounds__(kJumpBlockThreads, 1) ruler_jump_block(uint4* 
 // ---------------------------------------------------------------------------
 constexpr uint32_t kSuperLog2 = 4;
 
+// Rulers [rlo, rhi) are this call's (ruler_range); their super-rulers are
+// the multiples of 2^kSuperLog2 among them.
 __device__ __forceinline__ void ruler_super_walk_run(Grid grid, const uint4* __restrict__ state,
-    uint32_t rulers, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
+    uint32_t rlo, uint32_t rhi, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
     uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
         return; // the level is coloured by union-find
     }
-    const uint32_t supers = (rulers + (1u << kSuperLog2) - 1) >> kSuperLog2;
+    const uint32_t slo = (rlo + (1u << kSuperLog2) - 1) >> kSuperLog2;
+    const uint32_t shi = (rhi + (1u << kSuperLog2) - 1) >> kSuperLog2;
     uint64_t first = 0;
-    while (claim_chunk(control + kCtlClaimSuper, blockDim.x, supers, &first)) {
-        const uint64_t i = first + threadIdx.x;
-        if (i >= supers) {
+    while (claim_chunk(control + kCtlClaimSuper, blockDim.x, shi - slo, &first)) {
+        const uint64_t i = slo + first + threadIdx.x;
+        if (i >= shi) {
             continue;
         }
         const uint32_t r = (uint32_t)i << kSuperLog2;
@@ -491,7 +521,7 @@ __device__ __forceinline__ void ruler_super_walk_run(Grid grid, const uint4* __r
         super_of[r] = r;
         uint32_t ma = me.y, mb = me.z, cur = me.x;
         for (uint32_t hop = 0; (cur & ((1u << kSuperLog2) - 1)) != 0; ++hop) {
-            if (cur >= rulers || hop == kWalkCap) {
+            if (cur < rlo || cur >= rhi || hop == kWalkCap) {
                 atomicOr(control + kCtlHard, 1u);
                 break;
             }
@@ -506,20 +536,20 @@ __device__ __forceinline__ void ruler_super_walk_run(Grid grid, const uint4* __r
 }
 
 __global__ void __launch_bounds__(256) ruler_super_walk(const uint4* __restrict__ state,
-    uint32_t rulers, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
+    uint32_t rlo, uint32_t rhi, uint4* __restrict__ sstate, uint32_t* __restrict__ super_of,
     uint32_t* control) {
-    ruler_super_walk_run(launch_grid(), state, rulers, sstate, super_of, control);
+    ruler_super_walk_run(launch_grid(), state, rlo, rhi, sstate, super_of, control);
 }
 
 // Ruler cycles that contain no super-ruler: thread per ruler no super walk
 // reached; the ruler with the smallest id of its cycle folds the cycle's
 // minima and stamps the colour on every ruler of it.
 __device__ __forceinline__ void ruler_super_short_run(Grid grid, const uint4* __restrict__ state,
-    uint32_t rulers, uint32_t* __restrict__ super_of, uint32_t* control) {
+    uint32_t rlo, uint32_t rhi, uint32_t* __restrict__ super_of, uint32_t* control) {
     if (*(volatile uint32_t*)(control + kCtlHard) != 0) {
         return;
     }
-    for (uint32_t r = grid.bid * blockDim.x + threadIdx.x; r < rulers;
+    for (uint32_t r = rlo + grid.bid * blockDim.x + threadIdx.x; r < rhi;
          r += grid.nblk * blockDim.x) {
         if (super_of[r] != kUnset) {
             continue;
@@ -531,7 +561,7 @@ __device__ __forceinline__ void ruler_super_short_run(Grid grid, const uint4* __
         uint32_t ma = me.y, mb = me.z, cur = me.x;
         bool smallest = true, closed = false;
         for (uint32_t hop = 0; hop < kWalkCap; ++hop) {
-            if (cur >= rulers) {
+            if (cur < rlo || cur >= rhi) {
                 break;
             }
             if (cur == r) {
@@ -560,7 +590,7 @@ __device__ __forceinline__ void ruler_super_short_run(Grid grid, const uint4* __
         for (uint32_t hop = 0; hop < kWalkCap; ++hop) {
             super_of[cur] = colour;
             cur = state[cur].x;
-            if (cur == r || cur >= rulers) {
+            if (cur == r || cur < rlo || cur >= rhi) {
                 break;
             }
         }
@@ -568,8 +598,8 @@ __device__ __forceinline__ void ruler_super_short_run(Grid grid, const uint4* __
 }
 
 __global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict__ state,
-    uint32_t rulers, uint32_t* __restrict__ super_of, uint32_t* control) {
-    ruler_super_short_run(launch_grid(), state, rulers, super_of, control);
+    uint32_t rlo, uint32_t rhi, uint32_t* __restrict__ super_of, uint32_t* control) {
+    ruler_super_short_run(launch_grid(), state, rlo, rhi, super_of, control);
 }
 
 // After the jumping: every ruler's colour, stamped into super_of in place
@@ -577,14 +607,14 @@ __global__ void __launch_bounds__(256) ruler_super_short(const uint4* __restrict
 // super-ruler already have), so level_finalize resolves a vertex's owner
 // with one dependent load instead of two.  The super-ruler states read here
 // are the buffer the last jumping round wrote (kCtlFinal).
-__device__ __forceinline__ void ruler_colour_run(Grid grid, uint32_t rulers,
+__device__ __forceinline__ void ruler_colour_run(Grid grid, uint32_t rlo, uint32_t rhi,
     uint32_t* __restrict__ super_of, const uint4* __restrict__ s0, const uint4* __restrict__ s1,
     const uint32_t* control) {
     if (*(volatile const uint32_t*)(control + kCtlHard) != 0) {
         return; // the level is coloured by union-find
     }
     const uint4* state = control[kCtlFinal] ? s1 : s0;
-    for (uint32_t r = grid.bid * blockDim.x + threadIdx.x; r < rulers;
+    for (uint32_t r = rlo + grid.bid * blockDim.x + threadIdx.x; r < rhi;
          r += grid.nblk * blockDim.x) {
         const uint32_t so = super_of[r];
         if (so == kUnset || (so & kColourTag) != 0) {
@@ -595,9 +625,9 @@ __device__ __forceinline__ void ruler_colour_run(Grid grid, uint32_t rulers,
     }
 }
 
-__global__ void __launch_bounds__(256) ruler_colour(uint32_t rulers, uint32_t* super_of,
-    const uint4* s0, const uint4* s1, const uint32_t* control) {
-    ruler_colour_run(launch_grid(), rulers, super_of, s0, s1, control);
+__global__ void __launch_bounds__(256) ruler_colour(uint32_t rlo, uint32_t rhi,
+    uint32_t* super_of, const uint4* s0, const uint4* s1, const uint32_t* control) {
+    ruler_colour_run(launch_grid(), rlo, rhi, super_of, s0, s1, control);
 }
 
 // Clears the level's control words; `force_union_find` pre-sets the hard
@@ -628,7 +658,13 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
     const uint32_t ccap = (uint32_t)plan->levels[level + 1].cap;
-    const uint64_t total = (uint64_t)pcap << level;
+    // this call's pair-nodes [lo_pair, end); chunks start at a 32-pair
+    // boundary at or below lo_pair so colour words are written whole
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t lo_pair = nr.lo * pcap;
+    const uint64_t end = lo_pair + ((uint64_t)pcap << nr.shift);
+    const uint64_t begin = lo_pair & ~31ull;
+    const uint64_t total = end - begin;
     const bool hard = control[kCtlHard] != 0;
     const uint4* state = control[kCtlFinal] ? state1 : state0;
     const uint32_t lane = threadIdx.x & 31;
@@ -655,7 +691,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
         return first < total;
     };
     while (next_chunk()) {
-        const uint64_t p0 = first + (uint64_t)threadIdx.x * kResolveItems;
+        const uint64_t p0 = begin + first + (uint64_t)threadIdx.x * kResolveItems;
         uint32_t j = (uint32_t)(p0 / pcap);
         uint32_t k = (uint32_t)(p0 - (uint64_t)j * pcap);
         uint32_t s = size_at(lv, level, j);
@@ -667,7 +703,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
             kk[q] = k;
             ss[q] = s;
             c[q] = 0;
-            if (p0 + q < total && k < s - s / 2) live |= 1u << q;
+            if (p0 + q >= lo_pair && p0 + q < end && k < s - s / 2) live |= 1u << q;
             if (++k == pcap) {
                 k = 0;
                 ++j;
@@ -750,7 +786,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
         v |= __shfl_xor_sync(0xffffffffu, v, 1);
         v |= __shfl_xor_sync(0xffffffffu, v, 2);
         v |= __shfl_xor_sync(0xffffffffu, v, 4);
-        if ((lane & 7) == 0 && p0 < total) {
+        if ((lane & 7) == 0 && p0 < end) {
             xbits[p0 >> 5] = v;
         }
     }

@@ -79,6 +79,23 @@ int bpb200_compress_device(const void* d_entries, uint64_t count, uint32_t entry
     const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, void* stream,
     double* device_seconds, char* err, size_t err_len);
 
+/* Subtree sharding of one permutation over `shards` (a power of two) GPUs
+ * or calls; no reference counterpart (the reference splits the same
+ * recursion across host threads, src/benes.cpp:317-350).  With k =
+ * log2(shards), every shard runs routing levels 0..k-1 in full (they need
+ * the whole permutation; no exchange step) and, from level k on, only the
+ * subtree of level-k node `shard`, the 2^(l-k) consecutive nodes of each
+ * level l below it, through to their middle-group ranks.  Shard 0 alone
+ * writes levels 0..k-1's switches and the header; every other bit of the
+ * blob belongs to exactly one shard, so the byte-wise sum (or OR) of the
+ * shards' blobs is the whole blob, byte-identical to bpb200_compress_device.
+ * Same arguments as bpb200_compress_device otherwise; INVALID_ARGUMENT when
+ * shards is not a power of two, shard >= shards, or the permutation has
+ * fewer global routing levels than k. */
+int bpb200_compress_device_shard(const void* d_entries, uint64_t count, uint32_t entry_bytes,
+    const bpb200_format* format, uint8_t* d_blob, uint64_t blob_len, uint32_t shard,
+    uint32_t shards, void* stream, double* device_seconds, char* err, size_t err_len);
+
 /* Allocation-free form of bpb200_compress_device.  No counterpart in the
  * reference: its backends all allocate per call.  For callers that cannot
  * call cudaMalloc: processes whose device memory belongs to a pooling

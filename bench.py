@@ -80,6 +80,9 @@ def parse_args():
                     help="headline run without the serving sub-object")
     ap.add_argument("--max-log2", type=int, default=24, help="serving: largest log2 N")
     ap.add_argument("--hbm-budget", type=int, default=120 * 10**9, help="serving: admission budget")
+    ap.add_argument("--shard", action="store_true",
+                    help="N>1: one permutation sharded by subtrees over the ranks (strong "
+                         "scaling) instead of one replica per rank")
     ap.add_argument("--workers", type=int, default=4,
                     help="serving: concurrent workers for requests above one tile")
     return ap.parse_args()
@@ -91,7 +94,7 @@ def workload(log2n):
     return 1 << log2n, fmt
 
 
-def workload_config(n, log2n, world):
+def workload_config(n, log2n, world, shard_mode=False):
     return {
         "workload": f"compress uniform random permutation, N=2^{log2n} uint64, m=5, "
                     "default clusters, embedded_output",
@@ -99,7 +102,9 @@ def workload_config(n, log2n, world):
         "middle_placement": "embedded_output",
         "permutation": "Fisher-Yates, xoshiro256** seeded by splitmix64(0x5EED2030)",
         "l2": "inputs larger than L2 (8 GiB per step), no flush",
-        "parallelism": f"replicas x{world} (the path does not shard)",
+        "parallelism": (f"subtree shards x{world} of one permutation (top log2 N levels on "
+                        "every rank, shard blobs summed on rank 0)" if shard_mode else
+                        f"replicas x{world} (one permutation per rank)"),
     }
 
 
@@ -427,14 +432,23 @@ def b200_arm(args, world, rank, local):
     size = bp.encoded_size(n, fmt)
     depth, tile = bp.describe(n, fmt)
 
+    # --shard: every rank holds the same permutation and encodes its subtree
+    # shard (bpb200_compress_device_shard); the shards are summed on rank 0
+    shard_mode = args.shard and world > 1
+    seed = SEED if shard_mode else replica_seed(rank)
     host = torch.empty(n, dtype=torch.int64, pin_memory=True)
     perm = host.numpy().view(np.uint64)
-    bp.fill_permutation(bp.PermutationKind.uniform, replica_seed(rank), n, np.uint64, out=perm)
+    bp.fill_permutation(bp.PermutationKind.uniform, seed, n, np.uint64, out=perm)
     d_in = host.to(f"cuda:{local}", non_blocking=False)
     d_blob = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
 
     def step():
+        if shard_mode:
+            bp.compress_device_shard(d_in.data_ptr(), n, 8, d_blob.data_ptr(), size, rank, world,
+                                     fmt, stream.cuda_stream)
+            bp.combine_shards(d_blob)
+            return None
         return bp.compress_device(d_in.data_ptr(), n, 8, d_blob.data_ptr(), size, fmt,
                                   stream.cuda_stream)
 
@@ -483,13 +497,22 @@ def b200_arm(args, world, rank, local):
     if dist is not None:
         dist.barrier()
     secs = max_over_ranks(start.elapsed_time(stop) / 1e3, dist, f"cuda:{local}")
-    value = replica_throughput(n, args.steps, world, secs)
+    jobs = 1 if shard_mode else world  # permutations the whole job compresses per step
+    value = replica_throughput(n, args.steps, jobs, secs)
 
     # end to end through the host entry point: pinned input in, pinned blob out
     host_blob = torch.empty(size, dtype=torch.uint8, pin_memory=True)
     blob_np = host_blob.numpy()
     opts = bp.CompressOptions(format=fmt)
-    bp.compress(perm, opts, out=blob_np)
+    def host_call():
+        if shard_mode:
+            got = bp.compress_sharded(perm, opts)
+            if got is not None:
+                blob_np[:] = np.frombuffer(got, dtype=np.uint8)
+        else:
+            bp.compress(perm, opts, out=blob_np)
+
+    host_call()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
@@ -497,14 +520,17 @@ def b200_arm(args, world, rank, local):
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.e2e_steps):
-        bp.compress(perm, opts, out=blob_np)
+        host_call()
     e1.record(stream)
     torch.cuda.synchronize()
     e2e_secs = max_over_ranks(e0.elapsed_time(e1) / 1e3, dist, f"cuda:{local}")
-    e2e_value = replica_throughput(n, args.e2e_steps, world, e2e_secs)
+    e2e_value = replica_throughput(n, args.e2e_steps, jobs, e2e_secs)
 
-    verified = verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream,
-                             reference_digest(n, replica_seed(rank)))
+    if shard_mode and rank != 0:
+        verified = {"ok": True, "note": "shard mode: rank 0 holds and checks the combined blob"}
+    else:
+        verified = verify_output(bp, torch, d_in, d_blob, host_blob, n, size, fmt, stream,
+                                 reference_digest(n, seed))
     if not verified["ok"]:
         print(f"rank {rank}: the measured blob failed verification: {verified}",
               file=sys.stderr, flush=True)
@@ -552,8 +578,9 @@ def b200_arm(args, world, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": secs / args.steps * 1e3,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "uint64",
-        "data": "synthetic", "config": workload_config(n, args.log2n, world),
+        "higher_is_better": True, "scaling": "strong" if shard_mode else "weak",
+        "vs_baseline": None, "dtype": "uint64",
+        "data": "synthetic", "config": workload_config(n, args.log2n, world, shard_mode),
         "clocks": clocks.summary(),
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * 8,
                 "d2h_bytes_per_step": size, "steps": args.e2e_steps},

@@ -239,10 +239,8 @@ TileShape tile_shape(const Plan& p, uint32_t t0) {
     TileShape s;
     s.slots = (uint32_t)std::min<uint64_t>(slots, 1u << 30);
     s.pairs = (uint32_t)std::min<uint64_t>(pairs, 1u << 30);
-    uint32_t off[10];
-    const uint32_t depth_below = p.depth - t0;
-    s.smem = depth_below < 24 ? tile_smem_layout(s.slots, s.pairs, 1u << depth_below, off)
-                              : UINT32_MAX;
+    uint32_t off[9];
+    s.smem = tile_smem_layout(s.slots, s.pairs, off);
     if (slots >= 65536 || pairs >= (1u << 30)) {
         s.smem = UINT32_MAX;
     }

@@ -3,22 +3,7 @@
 // Tile kernel: one CTA per node of the tile level; the node's whole subtree
 // (every remaining routing level plus the middle-group ranks) is encoded in
 // shared memory.  Node-local values fit 16 bits (a tile holds at most a few
-// thousand entries).
-//
-// Colouring by pointer doubling.  With f(v) = inv[p[v^1]^1] (the orbit
-// successor of walk.cuh, with the virtual vertex s of an odd node) the
-// canonical colour is colour(v) = [min key(O(v)) > min key(O(v^1))],
-// key(tail) = 0, key(v) = v + 1 (src/benes.cpp:253-297).  Each vertex holds
-// one 32-bit word (min key << 16 | next): the minimum key over the orbit
-// segment from v up to, not including, `next`.  A round replaces a word
-// by the concatenation of its segment and the segment of its `next`, so
-// after r rounds every segment spans at least 2^r vertices and after
-// ceil(log2(s + 1)) rounds it covers the whole orbit.  Each word is read and
-// written whole, so a round may read a neighbour already updated in the
-// same round (a longer segment, still a true one); the barrier between
-// rounds guarantees the doubling.  No atomics, no data-dependent loops:
-// shared-memory union-find spent most of the tile's time in divergent finds
-// and failed links.
+// thousand entries), union-find words are 32-bit shared-memory words.
 #pragma once
 
 #include "device.cuh"
@@ -30,8 +15,6 @@
 namespace bpb200 {
 
 __host__ __device__ inline uint32_t align_up(uint32_t x, uint32_t a) { return (x + a - 1) / a * a; }
-
-
 
 // Division by a per-level constant: floor(n / d) = umulhi(n, ceil(2^32 / d))
 // exactly whenever n * d < 2^32 (the rounding error n * (m - 2^32/d) / 2^32
@@ -46,22 +29,19 @@ struct FastDiv {
 };
 
 // Byte offsets of the smem arrays; identical on host (sizing) and device.
-// `nodes`: the most nodes one tile level holds (2^(depth - tile level)),
-// the words of odd nodes' virtual vertices.
 __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pairs,
-    uint32_t nodes, uint32_t* off) {
+    uint32_t* off) {
     const uint32_t words = (pairs + 31) / 32 + 1;
     uint32_t o = 0;
     off[0] = o; o = align_up(o + slots * 2, 16);           // vals[0]
     off[1] = o; o = align_up(o + slots * 2, 16);           // vals[1]
     off[2] = o; o = align_up(o + slots * 2, 16);           // inv[0]
-    off[3] = o; o = align_up(o + slots * 4, 16);           // doubling words
+    off[3] = o; o = align_up(o + pairs * 4, 16);           // uf
     off[4] = o; o = align_up(o + words * 4, 16);           // xbits (input switches)
     off[5] = o; o = align_up(o + words * 4, 16);           // ybits (output switches)
     off[6] = o; o = align_up(o + 2 * kNodeWave * (uint32_t)sizeof(NodeAddress), 16);
     off[7] = o; o = align_up(o + kNodeWave * 8, 16);       // leafbit
     off[8] = o; o = align_up(o + slots * 2, 16);           // inv[1]
-    off[9] = o; o = align_up(o + nodes * 4, 16);           // virtual vertices' words
     return o;
 }
 
@@ -69,12 +49,11 @@ template <typename T>
 __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
     uint32_t pairs, uint32_t tile, unsigned char* smem) {
-    uint32_t off[10];
-    tile_smem_layout(slots, pairs, 1u << (plan_ptr->depth - plan_ptr->tile_level), off);
+    uint32_t off[9];
+    tile_smem_layout(slots, pairs, off);
     uint16_t* vals[2] = {(uint16_t*)(smem + off[0]), (uint16_t*)(smem + off[1])};
     uint16_t* invs[2] = {(uint16_t*)(smem + off[2]), (uint16_t*)(smem + off[8])};
-    uint32_t* words = (uint32_t*)(smem + off[3]);
-    uint32_t* vwords = (uint32_t*)(smem + off[9]);
+    uint32_t* uf = (uint32_t*)(smem + off[3]);
     uint32_t* xbits = (uint32_t*)(smem + off[4]);
     uint32_t* ybits = (uint32_t*)(smem + off[5]);
     NodeAddress* desc = (NodeAddress*)(smem + off[6]);
@@ -139,14 +118,19 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 }
                 __syncthreads();
             }
-            // A (first tile level only; every later level's inverse comes
-            // from its parent's phase E0): inverse
+            // A (first tile level only; every later level's inverse and
+            // union-find roots come from its parent's phase E0): inverse
+            // and union-find init
             for (uint32_t e = tid; t == 0 && e < nodes * cap; e += blockDim.x) {
                 const uint32_t path = by_cap(e);
                 const uint32_t i = e - path * cap;
                 const uint32_t s = size_at(lv, level, first + path);
                 if (i >= s || !internal_node(path, s)) {
                     continue;
+                }
+                if ((i & 1u) == 0) { // every pair-node is a root, whatever its values
+                    const uint32_t id = path * pcap + (i >> 1);
+                    uf[id] = id << 1;
                 }
                 const uint32_t v = cur[e];
                 if (v >= s) {
@@ -156,64 +140,42 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 inv[path * cap + v] = (uint16_t)i;
             }
             __syncthreads();
-            // B: every vertex's first word: its key and its successor f(v);
-            // an odd node's virtual vertex s keeps its word in vwords
-            auto successor = [&](uint32_t path, uint32_t s, uint32_t v) -> uint32_t {
-                const bool odd = (s & 1u) != 0;
-                const uint32_t node = path * cap;
-                const uint32_t a = v ^ 1u;
-                const uint32_t o = (odd && a == s) ? s : (uint32_t)cur[node + a];
-                const uint32_t b = o ^ 1u;
-                const uint32_t w = (odd && b == s) ? s : (b < s ? (uint32_t)inv[node + b] : 0xffffu);
-                if (w > s || (w == s && !odd)) { // only for a non-permutation
-                    atomicOr(status, kErrNotPermutation);
-                    return v;
-                }
-                return w;
-            };
-            for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
-                const uint32_t path = by_cap(e);
-                const uint32_t v = e - path * cap;
+            // B: one union per output pair.  Consecutive threads take the
+            // same pair of consecutive nodes, so the unions running at once
+            // spread over all nodes of the level instead of crowding one
+            // node's few roots (with 16 nodes of 256 pair-nodes, node-major
+            // order ran all 256 unions of a node at once; tile time at 2^30
+            // entries 157 -> 145 ms).
+            for (uint32_t idx = tid; idx < nodes * pcap; idx += blockDim.x) {
+                const uint32_t path = idx & (nodes - 1);
+                const uint32_t k = idx >> t;
                 const uint32_t s = size_at(lv, level, first + path);
-                if (v >= s || !internal_node(path, s)) {
+                if (k >= s / 2 || !internal_node(path, s)) {
                     continue;
                 }
-                const uint32_t key = ((s & 1u) != 0 && v == s - 1) ? 0u : v + 1;
-                words[e] = (key << 16) | successor(path, s, v);
+                const uint32_t u = inv[path * cap + 2 * k];
+                const uint32_t w = inv[path * cap + 2 * k + 1];
+                if (u >= s || w >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                    continue;
+                }
+                const uint32_t base = path * pcap;
+                uf_union(uf, base + (u >> 1), base + (w >> 1), 1u ^ (u & 1u) ^ (w & 1u), status);
             }
+            __syncthreads();
+            // C: orient odd nodes so the unpaired tail gets colour 0
             for (uint32_t path = tid; path < nodes; path += blockDim.x) {
                 const uint32_t s = size_at(lv, level, first + path);
-                if ((s & 1u) != 0 && internal_node(path, s)) {
-                    vwords[path] = ((s + 1) << 16) | successor(path, s, s);
+                if ((s & 1u) == 0 || !internal_node(path, s)) {
+                    continue;
                 }
-            }
-            // C: doubling rounds; the largest node of the level has at most
-            // cap entries, so its orbits at most cap + 1 vertices
-            uint32_t rounds = 0;
-            while ((1u << rounds) < cap + 1) ++rounds;
-            for (uint32_t r = 0; r < rounds; ++r) {
-                __syncthreads();
-                for (uint32_t e = tid; e < nodes * cap; e += blockDim.x) {
-                    const uint32_t path = by_cap(e);
-                    const uint32_t v = e - path * cap;
-                    const uint32_t s = size_at(lv, level, first + path);
-                    if (v >= s || !internal_node(path, s)) {
-                        continue;
-                    }
-                    const uint32_t w = words[e];
-                    const uint32_t nx = w & 0xffffu;
-                    const uint32_t wn = nx < s ? words[path * cap + nx] : vwords[path];
-                    words[e] = (min(w >> 16, wn >> 16) << 16) | (wn & 0xffffu);
+                if (inv[path * cap + s - 1] >= s) {
+                    atomicOr(status, kErrNotPermutation);
+                    continue;
                 }
-                for (uint32_t path = tid; path < nodes; path += blockDim.x) {
-                    const uint32_t s = size_at(lv, level, first + path);
-                    if ((s & 1u) == 0 || !internal_node(path, s)) {
-                        continue;
-                    }
-                    const uint32_t w = vwords[path];
-                    const uint32_t nx = w & 0xffffu;
-                    const uint32_t wn = nx < s ? words[path * cap + nx] : w;
-                    vwords[path] = (min(w >> 16, wn >> 16) << 16) | (wn & 0xffffu);
+                const Found f = uf_find(uf, path * pcap + (s >> 1), status);
+                if (f.bit) {
+                    atomicOr(uf + f.root, 1u);
                 }
             }
             __syncthreads();
@@ -228,12 +190,9 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     const uint32_t k = p - path * pcap;
                     const uint32_t s = size_at(lv, level, first + path);
                     if (k < s - s / 2 && internal_node(path, s)) {
-                        // colour(2k): orbit minimum of 2k against its mirror's
+                        const Found f = uf_find(uf, p, status);
+                        x = f.bit ^ (uf_load(uf, f.root) & 1u);
                         const uint32_t node = path * cap;
-                        const uint32_t mine = words[node + 2 * k] >> 16;
-                        const uint32_t mirror =
-                            (2 * k + 1 < s ? words[node + 2 * k + 1] : vwords[path]) >> 16;
-                        x = mine > mirror ? 1u : 0u;
                         const uint32_t half = s / 2;
                         if (k < half) {
                             nxt[2 * path * ccap + k] = (uint16_t)(cur[node + 2 * k + x] >> 1);
@@ -250,9 +209,10 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             }
             __syncthreads();
             // E0: output switch bits in natural order, and the children's
-            // inverse (as level_outputs does for the global levels: output
-            // pair k's colour-0 input inv[2k + y] goes left with value k, the
-            // other right)
+            // inverse and union-find roots (as level_outputs does for the
+            // global levels: output pair k's colour-0 input inv[2k + y]
+            // goes left with value k, the other right)
+            const uint32_t ccpcap = (uint32_t)plan.levels[level + 1].pcap;
             for (uint32_t base = warp * 32; base < ptotal; base += nwarps * 32) {
                 const uint32_t p = base + lane;
                 bool y = false;
@@ -279,6 +239,16 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                         } else if ((s & 1u) != 0) {
                             const uint32_t u = inv[path * cap + s - 1];
                             child_inv[lb + half] = u < s ? (uint16_t)(u >> 1) : (uint16_t)0xffffu;
+                        }
+                        if ((k & 1u) == 0) {
+                            if (k < s - half) {
+                                const uint32_t id = 2 * path * ccpcap + (k >> 1);
+                                uf[id] = id << 1;
+                            }
+                            if (k < half) {
+                                const uint32_t id = (2 * path + 1) * ccpcap + (k >> 1);
+                                uf[id] = id << 1;
+                            }
                         }
                     }
                 }
@@ -468,9 +438,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
     tile_body<T>(plan, src, blob, status, slots, pairs, first + blockIdx.x, smem);
 }
 
-// Tiles too large for two CTAs per SM (nodes of 16384 entries, about 200 KB
-// of shared memory): one CTA of twice the threads per SM keeps the same
-// number of resident warps.
+// Tiles too large for two CTAs per SM (nodes of 16384 entries, up to about
+// 200 KB of shared memory): one CTA of twice the threads per SM keeps the
+// same number of resident warps.
 template <typename T>
 __global__ void __launch_bounds__(2 * kTileThreads, 1) tile_encode_wide(
     const Plan* __restrict__ plan, const T* __restrict__ src, uint32_t* __restrict__ blob,

@@ -104,13 +104,14 @@ def main(argv) -> None:
     ref, oracle = Reference(), Oracle()
     threads = ref.hardware_threads()
     for name in names:
-        d = load(out)
         if name in SINGLE:
-            d[name] = single(name, ref, oracle, threads)
+            made = single(name, ref, oracle, threads)
         elif name in STREAMS:
-            d[name] = stream(name, ref, oracle, threads)
+            made = stream(name, ref, oracle, threads)
         else:
             raise SystemExit(f"unknown set {name}")
+        d = load(out)  # read just before writing: other sets may have landed meanwhile
+        d[name] = made
         save(d, out)
         print(name, "done", flush=True)
 

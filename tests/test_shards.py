@@ -26,7 +26,7 @@ from helpers import b200_format
     (1 << 18, np.uint32, 0, dict()),
     (100_003, np.uint64, 1, dict(middle_group_log2=4, middle_placement=2)),
     ((1 << 20) + 5, np.uint32, 0, dict(middle_group_log2=3, middle_placement=1,
-                                       input_clusters=[2, 9, 5], output_clusters=[16])),
+                                       input_clusters=[2, 9, 7], output_clusters=[18])),
     ((1 << 23) + 4097, np.uint64, 0, dict(middle_group_log2=5, middle_placement=2)),
 ])
 def test_shards_sum_to_the_plain_blob(gpu, n, dtype, kind, kw):

@@ -258,7 +258,13 @@ __global__ void __launch_bounds__(256) batch_orient(const LevelJob* jobs, uint32
     level_orient_run(g, j->plan, j->level, j->inv, j->uf, j->control + kCtlHard, j->status);
 }
 
-__global__ void __launch_bounds__(256) batch_finalize(const LevelJob* jobs, uint32_t n) {
+// Resident blocks per SM of batch_finalize (its job lookup costs registers
+// that level_finalize does not need).
+#ifndef BPB200_BATCH_FINAL_MIN_BLOCKS
+#define BPB200_BATCH_FINAL_MIN_BLOCKS 4
+#endif
+
+__global__ void __launch_bounds__(256, BPB200_BATCH_FINAL_MIN_BLOCKS) batch_finalize(const LevelJob* jobs, uint32_t n) {
     Grid g;
     const LevelJob* j = level_job(jobs, n, kBFinalize, &g);
     if (g.bid >= g.nblk) return;

@@ -23,6 +23,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -70,7 +71,9 @@ void check(cudaError_t e, const char* what) {
 struct Workspace {
     int device = -1;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr; // early blob download of the host path
     cudaEvent_t start = nullptr, stop = nullptr;
+    cudaEvent_t early = nullptr;        // the blob's first cluster groups are final
     Plan* d_plan = nullptr;
     Plan* h_plan = nullptr;       // pinned staging for the plan upload
     uint32_t* d_status = nullptr;
@@ -121,7 +124,9 @@ struct Workspace {
         if (h_status) cudaFreeHost(h_status);
         if (start) cudaEventDestroy(start);
         if (stop) cudaEventDestroy(stop);
+        if (early) cudaEventDestroy(early);
         if (stream) cudaStreamDestroy(stream);
+        if (copy_stream) cudaStreamDestroy(copy_stream);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
         *this = Workspace();
     }
@@ -143,6 +148,8 @@ Workspace* acquire(int device) {
     check(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreate(&w->start), "cudaEventCreate");
     check(cudaEventCreate(&w->stop), "cudaEventCreate");
+    check(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreateWithFlags(&w->early, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaMalloc(&w->d_plan, sizeof(Plan)), "cudaMalloc(plan)");
     check(cudaMallocHost(&w->h_plan, sizeof(Plan)), "cudaMallocHost(plan)");
     check(cudaMalloc(&w->d_status, sizeof(uint32_t)), "cudaMalloc(status)");
@@ -674,9 +681,13 @@ void allow_tile_smem(const void* kernel) {
     done.emplace_back(kernel, dev);
 }
 
+// Called after the launches of each global level are enqueued.
+using LevelHook = std::function<void(uint32_t level)>;
+
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
-    const TileShape& shape, const Tuning& tune, const T* d_in, uint32_t* d_blob) {
+    const TileShape& shape, const Tuning& tune, const T* d_in, uint32_t* d_blob,
+    const LevelHook* after_level = nullptr) {
     const Plan* dp = w.d_plan;
     const uint32_t t0 = p.tile_level;
     if (t0 > 0) {
@@ -697,6 +708,9 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
                 child_inv);
         }
         cur32 = dst;
+        if (after_level != nullptr) {
+            (*after_level)(l);
+        }
     }
     rec.level = (int)t0;
     const uint64_t tiles = 1ull << level_nodes(p, t0).shift;
@@ -828,7 +842,8 @@ std::atomic<int> g_profiling{0};
 
 // Queues the whole encode on `st` and waits for it.
 int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t entry_bytes,
-    uint32_t* d_blob, double* device_seconds, char* err, size_t err_len) {
+    uint32_t* d_blob, double* device_seconds, char* err, size_t err_len,
+    const LevelHook* after_level = nullptr) {
     const Plan& p = *call.plan;
     ensure_scratch(w, p);
     Recorder rec;
@@ -846,10 +861,10 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h); });
     if (entry_bytes == 4) {
         launch_levels<uint32_t>(w, rec, st, p, call.shape, call.tune, (const uint32_t*)d_in,
-            d_blob);
+            d_blob, after_level);
     } else {
         launch_levels<uint64_t>(w, rec, st, p, call.shape, call.tune, (const uint64_t*)d_in,
-            d_blob);
+            d_blob, after_level);
     }
     check(cudaEventRecord(w.stop, st), "cudaEventRecord");
     check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
@@ -942,6 +957,42 @@ void ensure_staging(Workspace& w, uint64_t in_bytes, uint64_t blob_len) {
 namespace bpb200 {
 namespace {
 
+// Blob bytes that no level after `level` writes: the header and, in each
+// section, the packets of the section's first cluster group.  Those lead the
+// section (every later group's packets and the embedded ranks follow them,
+// see cluster_base), so the host path downloads them while the remaining
+// levels run.  False when a section has one group, or its first group
+// reaches into the tile levels.
+struct EarlyPart {
+    uint32_t level = 0;
+    uint64_t off[2] = {0, 0}, len[2] = {0, 0};
+};
+
+bool early_part(const Plan& p, EarlyPart* e) {
+    if (p.shards > 1) {
+        return false;
+    }
+    uint32_t last = 0;
+    for (int side = 0; side < 2; ++side) {
+        if (p.group_count[side] < 2) {
+            return false;
+        }
+        const GroupInfo& g = p.groups[side][0];
+        last = std::max(last, g.start + g.depth - 1);
+    }
+    if (last + 1 >= p.tile_level) {
+        return false;
+    }
+    // the single node of level 0 is small (r_0 = 0): its packets take
+    // group_bits[0]; the byte holding a group's last bit may be shared
+    e->level = last;
+    e->off[0] = 0;
+    e->len[0] = p.section_offset[0] + p.groups[0][0].group_bits[0] / 8;
+    e->off[1] = p.section_offset[1];
+    e->len[1] = p.groups[1][0].group_bits[0] / 8;
+    return true;
+}
+
 // Host-memory compress (bpb200_compress): upload, encode, download.
 int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
     const bpb200_format* format, uint8_t* blob, uint64_t blob_len, double* device_seconds,
@@ -981,20 +1032,78 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
         check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
             "input upload");
     }
-    rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len);
+    // Bytes [0, end) of the blob are the encoding; the first cluster groups
+    // go down on the copy stream (through the ring on a helper thread for a
+    // pageable blob) as soon as their last level is done.
+    const uint64_t end = std::min<uint64_t>(blob_len, call.plan->end_offset);
+    const unsigned char* d_bytes = (const unsigned char*)w.blob;
+    auto download = [&](uint64_t off, uint64_t len, cudaStream_t st) {
+        if (len == 0) {
+            return;
+        }
+        if (stage_out) {
+            if (!download_staged(
+                    [blob, off](const unsigned char* src, uint64_t n, uint64_t o) {
+                        std::memcpy(blob + off + o, src, n);
+                        return true;
+                    },
+                    len, d_bytes + off, *ring->r, st)) {
+                throw CudaFail{cudaErrorUnknown, "staged blob download"};
+            }
+        } else {
+            check(cudaMemcpyAsync(blob + off, d_bytes + off, len, cudaMemcpyDeviceToHost, st),
+                "blob download");
+        }
+    };
+    EarlyPart early;
+    const bool split = end == call.plan->end_offset && early_part(*call.plan, &early);
+    std::thread helper;
+    std::atomic<int> helper_failed{0};
+    struct Join {
+        std::thread& t;
+        ~Join() {
+            if (t.joinable()) t.join();
+        }
+    } join{helper};
+    const LevelHook hook = [&](uint32_t level) {
+        if (level != early.level) {
+            return;
+        }
+        check(cudaEventRecord(w.early, w.stream), "cudaEventRecord");
+        check(cudaStreamWaitEvent(w.copy_stream, w.early, 0), "cudaStreamWaitEvent");
+        if (!stage_out) {
+            download(early.off[0], early.len[0], w.copy_stream);
+            download(early.off[1], early.len[1], w.copy_stream);
+            return;
+        }
+        helper = std::thread([&] {
+            try {
+                download(early.off[0], early.len[0], w.copy_stream);
+                download(early.off[1], early.len[1], w.copy_stream);
+            } catch (const CudaFail&) {
+                helper_failed.store(1);
+            }
+        });
+    };
+    rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len,
+        split ? &hook : nullptr);
+    if (helper.joinable()) {
+        helper.join();
+    }
+    if (split) {
+        check(cudaStreamSynchronize(w.copy_stream), "cudaStreamSynchronize");
+    }
     if (rc != kOk) {
         return rc;
     }
-    if (stage_out) {
-        download_staged(
-            [blob](const unsigned char* src, uint64_t len, uint64_t off) {
-                std::memcpy(blob + off, src, len);
-                return true;
-            },
-            blob_len, (const unsigned char*)w.blob, *ring->r, w.stream);
+    if (helper_failed.load()) {
+        throw CudaFail{cudaErrorUnknown, "staged blob download"};
+    }
+    if (split) {
+        download(early.len[0], early.off[1] - early.len[0], w.stream);
+        download(early.off[1] + early.len[1], end - early.off[1] - early.len[1], w.stream);
     } else {
-        check(cudaMemcpyAsync(blob, w.blob, blob_len, cudaMemcpyDeviceToHost, w.stream),
-            "blob download");
+        download(0, end, w.stream);
     }
     check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
     return kOk;

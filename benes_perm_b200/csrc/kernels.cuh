@@ -58,7 +58,21 @@ constexpr int kInverseItems = BPB200_INVERSE_ITEMS; // slots per thread in level
 #define BPB200_UNION_MIN_BLOCKS 4
 #endif
 constexpr int kUnionItems = BPB200_UNION_ITEMS; // output pairs per thread in level_union
-constexpr int kResolveItems = 4; // pair-nodes per thread in level_finalize (a nibble per lane)
+// level_finalize shape: pair-nodes per thread (2, 4 or 8; 32 / items lanes
+// assemble one colour word) and the minimum resident blocks of 256 per SM.
+// 2 pair-nodes at 8 blocks measured fastest on B200 at 2^30 uniform entries
+// (finalize 115 ms per compress; 2 at 6 blocks: 120; 4 at 6 blocks: 144;
+// 4 at the compiler's choice of 4 blocks: 134; 8: 286): the finds are
+// latency-bound, so more resident warps beat more finds per thread.
+#ifndef BPB200_RESOLVE_ITEMS
+#define BPB200_RESOLVE_ITEMS 2
+#endif
+#ifndef BPB200_FINAL_MIN_BLOCKS
+#define BPB200_FINAL_MIN_BLOCKS 8
+#endif
+constexpr int kResolveItems = BPB200_RESOLVE_ITEMS;
+static_assert(kResolveItems == 2 || kResolveItems == 4 || kResolveItems == 8,
+    "level_finalize assembles colour words from 2, 4 or 8 bits per lane");
 
 struct TileShape {
     uint32_t slots;   // padded entry slots needed at the deepest level
@@ -167,7 +181,7 @@ __global__ void __launch_bounds__(256) level_inverse(const Plan* __restrict__ pl
 // is a permutation; an overfull window means a repeated value.
 // ---------------------------------------------------------------------------
 #ifndef BPB200_PLACE_LOG2
-#define BPB200_PLACE_LOG2 23
+#define BPB200_PLACE_LOG2 24
 #endif
 constexpr uint32_t kPlaceLog2 = BPB200_PLACE_LOG2; // slots per destination window (log2)
 constexpr uint32_t kMaxWindows = 2048;
@@ -312,7 +326,10 @@ __device__ __forceinline__ void level_union_run(Grid grid, const Plan* __restric
     const uint64_t total = (uint64_t)pcap << nr.shift;
     const uint64_t end = begin + total;
     uint64_t first;
-    while (claim_chunk(claims, (uint64_t)blockDim.x * kUnionItems, total, &first)) {
+    auto next = [&]() -> bool {
+        return claim_chunk(claims, (uint64_t)blockDim.x * kUnionItems, total, &first);
+    };
+    while (next()) {
         const uint64_t p0 = begin + first + (uint64_t)threadIdx.x * kUnionItems;
         if (p0 >= end) {
             continue;

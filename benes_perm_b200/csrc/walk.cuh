@@ -61,6 +61,7 @@ namespace bpb200 {
 #define BPB200_FINAL_STRIDE_LOG2 24
 #endif
 
+
 constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
 constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
 constexpr uint32_t kWalkChunk = 16;          // rulers claimed per warp at a time
@@ -643,10 +644,10 @@ __global__ void control_reset(uint32_t* control, uint32_t force_union_find) {
 }
 
 // Colours (from the walks, or from union-find when the level fell back),
-// children and the colour bitmap: thread per 4 pair-nodes.  Blocks claim
-// chunks in address order so the finds (or ruler-state reads) of a chunk
-// stay within the nodes it covers.  Every thread of a block runs every
-// claimed chunk (the colour bitmap is assembled with warp shuffles).
+// children and the colour bitmap: kResolveItems pair-nodes per thread.
+// Blocks claim chunks in address order so the finds (or ruler-state reads)
+// of a chunk stay within the nodes it covers.  Every thread of a block runs
+// every claimed chunk (the colour bitmap is assembled with warp shuffles).
 template <typename T>
 __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
@@ -764,11 +765,11 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
                 c[q] = colour ^ flip[q];
             }
         }
-        uint32_t nibble = 0;
+        uint32_t mine = 0; // this lane's kResolveItems colour bits
 #pragma unroll
         for (int q = 0; q < kResolveItems; ++q) {
             if (!(live & (1u << q))) continue;
-            nibble |= c[q] << q;
+            mine |= c[q] << q;
             const uint64_t node = (uint64_t)jj[q] * cap;
             const uint64_t left = (uint64_t)(2 * jj[q]) * ccap;
             const uint64_t right = (uint64_t)(2 * jj[q] + 1) * ccap;
@@ -782,18 +783,21 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
                 dst[left + kk[q]] = (uint32_t)(src[node + ss[q] - 1] >> 1);
             }
         }
-        uint32_t v = nibble << ((lane & 7) * 4);
-        v |= __shfl_xor_sync(0xffffffffu, v, 1);
-        v |= __shfl_xor_sync(0xffffffffu, v, 2);
-        v |= __shfl_xor_sync(0xffffffffu, v, 4);
-        if ((lane & 7) == 0 && p0 < end) {
+        // 32 / kResolveItems lanes hold one 32-pair colour word
+        constexpr uint32_t kWordLanes = 32 / kResolveItems;
+        uint32_t v = mine << ((lane & (kWordLanes - 1)) * kResolveItems);
+#pragma unroll
+        for (uint32_t d = 1; d < kWordLanes; d <<= 1) {
+            v |= __shfl_xor_sync(0xffffffffu, v, d);
+        }
+        if ((lane & (kWordLanes - 1)) == 0 && p0 < end) {
             xbits[p0 >> 5] = v;
         }
     }
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) level_finalize(const Plan* __restrict__ plan,
+__global__ void __launch_bounds__(256, BPB200_FINAL_MIN_BLOCKS) level_finalize(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, const uint32_t* __restrict__ owner,
     const uint32_t* __restrict__ super_of, const uint4* __restrict__ state0,
     const uint4* __restrict__ state1, uint32_t* uf,

@@ -146,6 +146,45 @@ def test_partitioned_inverse_levels(gpu, oracle):
     assert gpu.compress(perm, opts) == oracle.compress(perm, oracle_format(kw))
 
 
+def test_host_path_early_download(gpu, oracle):
+    # On inputs whose first cluster groups end above the tile levels (here
+    # 2^23 + 12345 entries: 20 or 19 routing levels, tiles from level 11),
+    # the host entry point downloads the header and those groups' packets
+    # while the lower levels run: on a copy stream into a pinned blob, through
+    # the staging ring on a helper thread into a pageable one.  Both must
+    # equal the device-resident path, and one format the oracle.
+    import torch
+    n = (1 << 23) + 12345
+    cases = [dict(middle_group_log2=4, middle_placement=0),
+             dict(middle_group_log2=5, middle_placement=2),
+             dict(middle_group_log2=4, middle_placement=1, input_clusters=[4, 7, 9],
+                  output_clusters=[10, 10]),
+             dict(middle_group_log2=5, middle_placement=0, input_clusters=[4, 7, 8],
+                  output_clusters=[10, 9])]
+    for i, kw in enumerate(cases):
+        dtype = np.uint64 if i % 2 else np.uint32
+        perm = gpu.fill_permutation(gpu.PermutationKind(i % 2), 0xE4 + i, n, dtype)
+        fmt = b200_format(gpu, kw)
+        size = gpu.encoded_size(n, fmt)
+        w = np.dtype(dtype).itemsize
+        d_in = torch.from_numpy(perm.view(np.int64 if w == 8 else np.int32)).cuda()
+        d_blob = torch.empty((size + 3) // 4 * 4, dtype=torch.uint8, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        gpu.compress_device(d_in.data_ptr(), n, w, d_blob.data_ptr(), size, fmt, stream)
+        torch.cuda.synchronize()
+        want = d_blob[:size].cpu().numpy().tobytes()
+        opts = gpu.CompressOptions(format=fmt)
+        assert gpu.compress(perm, opts) == want, kw
+        pinned = torch.zeros(size + 64, dtype=torch.uint8, pin_memory=True)
+        pinned[size:] = 0xA5
+        got = gpu.compress(perm, opts, out=pinned.numpy())
+        assert bytes(got) == want, kw
+        # bytes past the encoded size are left as they were
+        assert bool((pinned[size:] == 0xA5).all()), kw
+        if i == 2:
+            assert want == oracle.compress(perm, oracle_format(kw)), kw
+
+
 def test_invalid_inputs_then_recovery(gpu, oracle):
     for bad in ([0, 1, 1], [0, 1, 3], [5, 0, 1, 2, 3, 4, 4]):
         for dt in (np.uint32, np.uint64):

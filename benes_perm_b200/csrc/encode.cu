@@ -993,6 +993,21 @@ bool early_part(const Plan& p, EarlyPart* e) {
     return true;
 }
 
+// Narrowing of 64-bit host inputs before the upload (on unless the
+// environment sets BPB200_NARROW_UPLOAD=0), with up to 16 host threads.
+bool narrow_upload_enabled() {
+    static const bool on = [] {
+        const char* v = std::getenv("BPB200_NARROW_UPLOAD");
+        return v == nullptr || std::strcmp(v, "0") != 0;
+    }();
+    return on;
+}
+
+int narrow_threads() {
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(16u, hw));
+}
+
 // Host-memory compress (bpb200_compress): upload, encode, download.
 int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
     const bpb200_format* format, uint8_t* blob, uint64_t blob_len, double* device_seconds,
@@ -1011,16 +1026,46 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
     }
     const uint64_t in_bytes = count * entry_bytes;
     ensure_staging(w, in_bytes, blob_len);
-    // Pageable buffers of a few MB and more go through the pinned ring
-    // (parallel host copies overlapping the transfer); pinned ones and
-    // small ones are copied directly.
-    const bool stage_in = in_bytes >= kStageMin && !host_is_pinned(entries);
+    // 64-bit inputs of up to 2^32 entries cross PCIe as 32-bit values: the
+    // ring's threads narrow them while the copy engine moves the chunks
+    // already done, halving the bytes on the link.  Every valid value is
+    // below count <= 2^32; a wider one means the input is not a permutation.
+    const bool narrow = entry_bytes == 8 && count <= (1ull << 32) && in_bytes >= kStageMin &&
+        narrow_upload_enabled();
+    // Other pageable buffers of a few MB and more go through the pinned ring
+    // (parallel host copies overlapping the transfer); pinned ones and small
+    // ones are copied directly.
+    const bool stage_in = !narrow && in_bytes >= kStageMin && !host_is_pinned(entries);
     const bool stage_out = blob_len >= kStageMin && !host_is_pinned(blob);
     std::unique_ptr<RingLease> ring;
-    if (stage_in || stage_out) {
+    if (narrow || stage_in || stage_out) {
         ring = std::make_unique<RingLease>(device);
     }
-    if (stage_in) {
+    uint32_t device_width = entry_bytes;
+    if (narrow) {
+        const uint64_t* src = static_cast<const uint64_t*>(entries);
+        std::atomic<uint64_t> wide{0};
+        upload_staged(
+            [src, &wide](unsigned char* dst, uint64_t len, uint64_t off) {
+                uint32_t* out = reinterpret_cast<uint32_t*>(dst);
+                const uint64_t* in = src + off / 4;
+                const uint64_t n = len / 4;
+                uint64_t high = 0;
+                for (uint64_t i = 0; i < n; ++i) {
+                    high |= in[i];
+                    out[i] = (uint32_t)in[i];
+                }
+                if (high >> 32) wide.fetch_or(1);
+                return true;
+            },
+            count * 4, (unsigned char*)w.input, *ring->r, w.stream, narrow_threads());
+        if (wide.load() != 0) {
+            check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
+            set_error(err, err_len, "input must contain every value from zero through size minus one");
+            return kInvalidArgument;
+        }
+        device_width = 4;
+    } else if (stage_in) {
         const unsigned char* src = static_cast<const unsigned char*>(entries);
         upload_staged(
             [src](unsigned char* dst, uint64_t len, uint64_t off) {
@@ -1085,7 +1130,7 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
             }
         });
     };
-    rc = run(w, call, w.stream, w.input, entry_bytes, w.blob, device_seconds, err, err_len,
+    rc = run(w, call, w.stream, w.input, device_width, w.blob, device_seconds, err, err_len,
         split ? &hook : nullptr);
     if (helper.joinable()) {
         helper.join();

@@ -73,16 +73,32 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
         return; // child of a leaf: not part of the tree
     }
     {
+        // every load of a batch is issued before any is used: the error
+        // atomic below may alias the input as far as the compiler knows, so
+        // a plain loop would wait out one HBM round trip per element
         const LevelInfo& l0 = plan.levels[T0];
         const uint32_t s0 = size_at(l0, T0, J);
         const T* in = src + (uint64_t)J * l0.cap;
-        for (uint32_t i = tid; i < s0; i += blockDim.x) {
-            const uint64_t v = (uint64_t)in[i];
-            if (v >= s0) {
-                atomicOr(status, kErrNotPermutation);
-                vals[0][i] = 0;
-            } else {
-                vals[0][i] = (uint16_t)v;
+        constexpr int kBatch = 8;
+        for (uint32_t i0 = tid; i0 < s0; i0 += kBatch * blockDim.x) {
+            uint64_t v[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const uint32_t i = i0 + q * blockDim.x;
+                v[q] = i < s0 ? (uint64_t)__ldcs(in + i) : 0;
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q) {
+                const uint32_t i = i0 + q * blockDim.x;
+                if (i >= s0) {
+                    break;
+                }
+                if (v[q] >= s0) {
+                    atomicOr(status, kErrNotPermutation);
+                    vals[0][i] = 0;
+                } else {
+                    vals[0][i] = (uint16_t)v[q];
+                }
             }
         }
     }

@@ -722,22 +722,16 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
                 if (live & (1u << q)) c[q] = f[q].bit ^ (uf[f[q].root] & 1u);
             }
         } else {
-            // ruler id (or direct colour) of vertex 2k, else of 2k+1
-            uint32_t id[kResolveItems], flip[kResolveItems];
+            // ruler id (or direct colour) of vertex 2k: every even vertex is
+            // a ruler, stamped by the ruler walk that passes it, or stamped
+            // by the short walk of its ruler-free orbit (odd vertices are
+            // never read, and their owner slots are never reset)
+            uint32_t id[kResolveItems];
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {
                 if (!(live & (1u << q))) continue;
                 const uint32_t slot = jj[q] * cap + 2 * kk[q];
-                flip[q] = 0;
-                if (is_ruler_slot(slot)) {
-                    id[q] = slot >> kRulerLog2;
-                } else {
-                    id[q] = owner[slot];
-                    if (id[q] == kUnset && 2 * kk[q] + 1 < ss[q]) {
-                        flip[q] = 1;
-                        id[q] = is_ruler_slot(slot + 1) ? (slot + 1) >> kRulerLog2 : owner[slot + 1];
-                    }
-                }
+                id[q] = is_ruler_slot(slot) ? slot >> kRulerLog2 : owner[slot];
             }
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {
@@ -762,7 +756,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
                         colour = st.y > st.z ? 1u : 0u;
                     }
                 }
-                c[q] = colour ^ flip[q];
+                c[q] = colour;
             }
         }
         uint32_t mine = 0; // this lane's kResolveItems colour bits

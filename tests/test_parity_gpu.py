@@ -185,6 +185,29 @@ def test_host_path_early_download(gpu, oracle):
             assert want == oracle.compress(perm, oracle_format(kw)), kw
 
 
+def test_host_path_narrowed_upload(gpu, oracle):
+    # 64-bit host inputs of 4 MB and more cross PCIe as 32-bit values; a
+    # value of 2^32 or more must still be reported as a non-permutation, and
+    # a narrowed input must give the bytes of the 32-bit input.
+    import torch
+    n = (1 << 20) + 3
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 0x4A, n, np.uint64)
+    kw = dict(middle_group_log2=4, middle_placement=2)
+    opts = gpu.CompressOptions(format=b200_format(gpu, kw))
+    want = oracle.compress(perm, oracle_format(kw))
+    assert gpu.compress(perm, opts) == want
+    assert gpu.compress(perm.astype(np.uint32), opts) == want
+    pinned = torch.empty(n, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    pinned[:] = perm
+    assert gpu.compress(pinned, opts) == want
+    for bad_value in (1 << 32, (1 << 63) + 5, n):
+        bad = perm.copy()
+        bad[n // 2] = bad_value
+        with pytest.raises(ValueError, match="every value"):
+            gpu.compress(bad, opts)
+    assert gpu.compress(perm, opts) == want
+
+
 def test_invalid_inputs_then_recovery(gpu, oracle):
     for bad in ([0, 1, 1], [0, 1, 3], [5, 0, 1, 2, 3, 4, 4]):
         for dt in (np.uint32, np.uint64):

@@ -440,9 +440,11 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
 // and an odd node's tail output s - 1, whose input is coloured 0, gives
 // left_inv[s / 2] = inv[s - 1] >> 1.  The pass reads inv sequentially and
 // one colour bit per output pair, and writes the children's inverse
-// sequentially.  It also resets the children's walk owners (even slots only:
-// the walks read no others) and pair-node union-find roots (`child_owner` /
-// `child_uf`, may be null), the state the next level's colouring starts from.  A value out of range (only
+// sequentially.  It also resets the children's walk owners (every slot: the
+// walks read only even ones, but writing every other word turns each
+// 32-byte sector into a read-modify-write, measured 3.7 ms slower per
+// 2^30 compress) and pair-node union-find roots (`child_owner` / `child_uf`,
+// may be null), the state the next level's colouring starts from.  A value out of range (only
 // possible when the input was not a permutation, which level 0 reports)
 // leaves 0xffffffff, which every user range-checks.
 __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restrict__ plan,
@@ -487,14 +489,14 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
                     child_inv[lb + k] = to_left;
                     child_inv[rb + k] = to_right;
                 }
-                if (child_owner != nullptr && (k & 1u) == 0) { // walks read even slots only
+                if (child_owner != nullptr) {
                     child_owner[lb + k] = ~0u;
                     child_owner[rb + k] = ~0u;
                 }
             } else if (k == half && (s & 1u) != 0) {
                 const uint32_t u = inv[node + s - 1];
                 if (child_inv != nullptr) child_inv[lb + half] = u < s ? u >> 1 : ~0u;
-                if (child_owner != nullptr && (half & 1u) == 0) child_owner[lb + half] = ~0u;
+                if (child_owner != nullptr) child_owner[lb + half] = ~0u;
             }
             // children's pair-nodes start as their own roots: left child of
             // s - s/2 entries, right of s/2; pair-node k/2 for even k

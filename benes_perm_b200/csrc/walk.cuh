@@ -724,8 +724,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
         } else {
             // ruler id (or direct colour) of vertex 2k: every even vertex is
             // a ruler, stamped by the ruler walk that passes it, or stamped
-            // by the short walk of its ruler-free orbit (odd vertices are
-            // never read, and their owner slots are never reset)
+            // by the short walk of its ruler-free orbit
             uint32_t id[kResolveItems];
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {

@@ -45,6 +45,72 @@ __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pa
     return o;
 }
 
+// Tile input through one bulk asynchronous copy (1) or batched plain loads (0).
+#ifndef BPB200_TILE_BULK_LOAD
+#define BPB200_TILE_BULK_LOAD 0
+#endif
+constexpr uint32_t kBulkWaitCap = 1u << 22; // mbarrier polls before giving up
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bounded wait for phase 0 of `mbar`; true once the phase has completed.
+__device__ __forceinline__ bool bulk_wait(uint32_t mbar) {
+    for (uint32_t it = 0; it < kBulkWaitCap; ++it) {
+        uint32_t done = 0;
+        asm volatile("{\n\t.reg .pred p;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}"
+                     : "=r"(done) : "r"(mbar), "r"(0u) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+// Copies the s0 32-bit input values at `in` into `stage` (16-byte aligned,
+// at least s0 * 4 + 16 bytes, free until the caller is done with it): the
+// 16-byte-aligned interior of the range with one cp.async.bulk counted on an
+// mbarrier, the ragged ends (at most three values each) with plain loads, so
+// nothing outside the range is read.  Value i lands at stage[lead + i];
+// returns lead, or ~0u when the copy did not complete within the poll bound
+// (the status word then says so).  Every thread of the block calls it.
+__device__ __forceinline__ uint32_t tile_bulk_stage(const uint32_t* in, uint32_t s0,
+    uint32_t* stage, uint64_t* mbar, uint32_t* status) {
+    const uint64_t g0 = (uint64_t)in;
+    const uint64_t g1 = g0 + (uint64_t)s0 * 4;
+    const uint64_t a0 = (g0 + 15) & ~15ull;
+    const uint64_t a1 = g1 & ~15ull;
+    const uint32_t lead = (uint32_t)((g0 & 15) >> 2);
+    const bool bulk = a1 > a0;
+    const uint32_t mb = smem_addr(mbar);
+    if (threadIdx.x == 0 && bulk) {
+        const uint32_t bytes = (uint32_t)(a1 - a0);
+        const uint32_t dst = smem_addr(stage) + (uint32_t)(a0 - (g0 & ~15ull));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(mb) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(mb), "r"(bytes) : "memory");
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+                     "[%0], [%1], %2, [%3];"
+                     :: "r"(dst), "l"(a0), "r"(bytes), "r"(mb) : "memory");
+    }
+    // ragged ends: values before a0 and from a1 on (all of them without bulk)
+    const uint32_t head = bulk ? (uint32_t)((a0 - g0) >> 2) : s0;
+    const uint32_t tail = bulk ? (uint32_t)((a1 - g0) >> 2) : s0;
+    for (uint32_t i = threadIdx.x; i < head; i += blockDim.x) stage[lead + i] = in[i];
+    for (uint32_t i = tail + threadIdx.x; i < s0; i += blockDim.x) stage[lead + i] = in[i];
+    __syncthreads(); // the mbarrier is initialised before anyone polls it
+    const bool ok = !bulk || bulk_wait(mb);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(status, kErrIterationCap);
+        bulk_wait(mb); // give the copy in flight one more bounded chance
+        __syncthreads();
+        return ~0u;
+    }
+    return lead;
+}
+
 template <typename T>
 __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
@@ -73,14 +139,38 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
         return; // child of a leaf: not part of the tree
     }
     {
-        // every load of a batch is issued before any is used: the error
-        // atomic below may alias the input as far as the compiler knows, so
-        // a plain loop would wait out one HBM round trip per element
         const LevelInfo& l0 = plan.levels[T0];
         const uint32_t s0 = size_at(l0, T0, J);
         const T* in = src + (uint64_t)J * l0.cap;
+        bool loaded = false;
+#if BPB200_TILE_BULK_LOAD
+        if (sizeof(T) == 4 && s0 >= 256) {
+            // staged over vals[1], inv[0] and the union-find words, which
+            // phase A fills only after the conversion below
+            __shared__ uint64_t bulk_bar;
+            uint32_t* stage = (uint32_t*)(smem + off[1]);
+            const uint32_t lead = tile_bulk_stage((const uint32_t*)in, s0, stage, &bulk_bar,
+                status);
+            if (lead == ~0u) {
+                return;
+            }
+            for (uint32_t i = tid; i < s0; i += blockDim.x) {
+                const uint32_t v = stage[lead + i];
+                if (v >= s0) {
+                    atomicOr(status, kErrNotPermutation);
+                    vals[0][i] = 0;
+                } else {
+                    vals[0][i] = (uint16_t)v;
+                }
+            }
+            loaded = true;
+        }
+#endif
+        // every load of a batch is issued before any is used: the error
+        // atomic below may alias the input as far as the compiler knows, so
+        // a plain loop would wait out one HBM round trip per element
         constexpr int kBatch = 8;
-        for (uint32_t i0 = tid; i0 < s0; i0 += kBatch * blockDim.x) {
+        for (uint32_t i0 = tid; !loaded && i0 < s0; i0 += kBatch * blockDim.x) {
             uint64_t v[kBatch];
 #pragma unroll
             for (int q = 0; q < kBatch; ++q) {

@@ -56,15 +56,21 @@ namespace bpb200 {
 #endif
 // Union-find levels whose nodes have at most 2^BPB200_FINAL_STRIDE_LOG2
 // slots finalize in grid-stride order, larger ones in claimed order (see
-// level_finalize); measured on B200 at 2^30 uniform entries.
+// level_finalize); measured on B200 at 2^30 uniform entries (finalize 105 ms
+// per compress; limit 2^24: 110 ms; 2^23: 119 ms).
 #ifndef BPB200_FINAL_STRIDE_LOG2
-#define BPB200_FINAL_STRIDE_LOG2 24
+#define BPB200_FINAL_STRIDE_LOG2 26
 #endif
 
 
 constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
 constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
-constexpr uint32_t kWalkChunk = 16;          // rulers claimed per warp at a time
+#ifndef BPB200_WALK_CHUNK
+#define BPB200_WALK_CHUNK 32
+#endif
+// rulers claimed per warp at a time: 32 measured fastest on B200 at 2^30
+// uniform entries (walks 157 ms per compress; 16: 159 ms; 8: 176 ms)
+constexpr uint32_t kWalkChunk = BPB200_WALK_CHUNK;
 constexpr uint32_t kJumpItems = 8;           // rulers per thread in a claimed jump chunk
 constexpr uint64_t kWalkMaxNode = 1ull << BPB200_WALK_MAX_LOG2; // larger: union-find
 static_assert(BPB200_RULER_LOG2 >= 2 && BPB200_RULER_LOG2 <= 8, "ruler density out of range");

@@ -19,7 +19,9 @@
 #include <dlfcn.h>
 
 #include <algorithm>
+#include <array>
 #include <atomic>
+#include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -74,6 +76,7 @@ struct Workspace {
     cudaStream_t copy_stream = nullptr; // early blob download of the host path
     cudaEvent_t start = nullptr, stop = nullptr;
     cudaEvent_t early = nullptr;        // the blob's first cluster groups are final
+    cudaEvent_t parts[8] = {};          // tile parts done (progressive blob download)
     Plan* d_plan = nullptr;
     Plan* h_plan = nullptr;       // pinned staging for the plan upload
     uint32_t* d_status = nullptr;
@@ -125,6 +128,9 @@ struct Workspace {
         if (start) cudaEventDestroy(start);
         if (stop) cudaEventDestroy(stop);
         if (early) cudaEventDestroy(early);
+        for (cudaEvent_t e : parts) {
+            if (e) cudaEventDestroy(e);
+        }
         if (stream) cudaStreamDestroy(stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
@@ -150,6 +156,9 @@ Workspace* acquire(int device) {
     check(cudaEventCreate(&w->stop), "cudaEventCreate");
     check(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&w->early, cudaEventDisableTiming), "cudaEventCreate");
+    for (cudaEvent_t& e : w->parts) {
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    }
     check(cudaMalloc(&w->d_plan, sizeof(Plan)), "cudaMalloc(plan)");
     check(cudaMallocHost(&w->h_plan, sizeof(Plan)), "cudaMallocHost(plan)");
     check(cudaMalloc(&w->d_status, sizeof(uint32_t)), "cudaMalloc(status)");
@@ -684,10 +693,17 @@ void allow_tile_smem(const void* kernel) {
 // Called after the launches of each global level are enqueued.
 using LevelHook = std::function<void(uint32_t level)>;
 
+// The tile launch split into parts at ascending tile indices (`cuts`, the
+// last one the tile count), with a hook after each part's launch.
+struct TileParts {
+    std::vector<uint64_t> cuts;
+    std::function<void(uint32_t part)> after_part;
+};
+
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     const TileShape& shape, const Tuning& tune, const T* d_in, uint32_t* d_blob,
-    const LevelHook* after_level = nullptr) {
+    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr) {
     const Plan* dp = w.d_plan;
     const uint32_t t0 = p.tile_level;
     if (t0 > 0) {
@@ -720,10 +736,21 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     const bool wide = shape.smem > kTileSmemTwoPerSm;
     auto launch_tile = [&](auto kernel, const auto* src, unsigned threads) {
         allow_tile_smem((const void*)kernel);
-        rec.launch(kKindTile, [&] {
-            kernel<<<(unsigned)tiles, threads, shape.smem, st>>>(dp, src, d_blob, w.d_status,
-                shape.slots, shape.pairs);
-        });
+        uint64_t lo = 0;
+        const size_t count = parts != nullptr ? parts->cuts.size() : 1;
+        for (size_t k = 0; k < count; ++k) {
+            const uint64_t hi = parts != nullptr ? parts->cuts[k] : tiles;
+            if (hi > lo) {
+                rec.launch(kKindTile, [&] {
+                    kernel<<<(unsigned)(hi - lo), threads, shape.smem, st>>>(dp, src, d_blob,
+                        w.d_status, shape.slots, shape.pairs, (uint32_t)lo);
+                });
+            }
+            if (parts != nullptr && parts->after_part) {
+                parts->after_part((uint32_t)k);
+            }
+            lo = hi;
+        }
     };
     if (t0 == 0) {
         if (wide) {
@@ -843,7 +870,7 @@ std::atomic<int> g_profiling{0};
 // Queues the whole encode on `st` and waits for it.
 int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t entry_bytes,
     uint32_t* d_blob, double* device_seconds, char* err, size_t err_len,
-    const LevelHook* after_level = nullptr) {
+    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr) {
     const Plan& p = *call.plan;
     ensure_scratch(w, p);
     Recorder rec;
@@ -861,10 +888,10 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h); });
     if (entry_bytes == 4) {
         launch_levels<uint32_t>(w, rec, st, p, call.shape, call.tune, (const uint32_t*)d_in,
-            d_blob, after_level);
+            d_blob, after_level, parts);
     } else {
         launch_levels<uint64_t>(w, rec, st, p, call.shape, call.tune, (const uint64_t*)d_in,
-            d_blob, after_level);
+            d_blob, after_level, parts);
     }
     check(cudaEventRecord(w.stop, st), "cudaEventRecord");
     check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
@@ -957,40 +984,80 @@ void ensure_staging(Workspace& w, uint64_t in_bytes, uint64_t blob_len) {
 namespace bpb200 {
 namespace {
 
-// Blob bytes that no level after `level` writes: the header and, in each
-// section, the packets of the section's first cluster group.  Those lead the
-// section (every later group's packets and the embedded ranks follow them,
-// see cluster_base), so the host path downloads them while the remaining
-// levels run.  False when a section has one group, or its first group
-// reaches into the tile levels.
-struct EarlyPart {
+// Pieces of the blob that are final before the last launch, so the host
+// path downloads them while the remaining work runs.  A section lists, per
+// cluster group in order, each cluster's packets followed by the sections of
+// its child clusters (cluster_base), so:
+//  - after the last level of the first groups (the header and, per section,
+//    the level-0 cluster's packets: `level`, `first[]`), when both sections
+//    have more groups and those levels are all global;
+//  - when the last group of both sections starts at or above the tile level,
+//    after each of kTileParts tile launches: every byte before the first
+//    last-group cluster whose tiles have not run yet (`cuts`, `upto[k][]`).
+// The byte holding a piece's last bit may be shared with the next piece, so
+// pieces end at the byte below it.
+constexpr uint32_t kTileParts = 8;
+
+struct EarlyPlan {
+    bool levels = false;
     uint32_t level = 0;
-    uint64_t off[2] = {0, 0}, len[2] = {0, 0};
+    uint64_t first[2] = {0, 0};          // end of the first-group piece, per section
+    std::vector<uint64_t> cuts;          // tile part ends (empty: one launch)
+    std::vector<std::array<uint64_t, 2>> upto; // per part, per section: bytes final after it
 };
 
-bool early_part(const Plan& p, EarlyPart* e) {
-    if (p.shards > 1) {
-        return false;
+EarlyPlan early_plan(const Plan& p) {
+    EarlyPlan e;
+    if (p.shards > 1 || p.tile_level == 0) {
+        return e;
     }
     uint32_t last = 0;
+    bool multi = true;
     for (int side = 0; side < 2; ++side) {
         if (p.group_count[side] < 2) {
-            return false;
+            multi = false;
+            break;
         }
         const GroupInfo& g = p.groups[side][0];
         last = std::max(last, g.start + g.depth - 1);
     }
-    if (last + 1 >= p.tile_level) {
-        return false;
+    if (multi && last + 1 < p.tile_level) {
+        // the single node of level 0 is small (r_0 = 0): its packets take
+        // group_bits[0]
+        e.levels = true;
+        e.level = last;
+        e.first[0] = p.section_offset[0] + p.groups[0][0].group_bits[0] / 8;
+        e.first[1] = p.section_offset[1] + p.groups[1][0].group_bits[0] / 8;
     }
-    // the single node of level 0 is small (r_0 = 0): its packets take
-    // group_bits[0]; the byte holding a group's last bit may be shared
-    e->level = last;
-    e->off[0] = 0;
-    e->len[0] = p.section_offset[0] + p.groups[0][0].group_bits[0] / 8;
-    e->off[1] = p.section_offset[1];
-    e->len[1] = p.groups[1][0].group_bits[0] / 8;
-    return true;
+    uint32_t s_min = p.tile_level;
+    uint32_t glast[2], slast[2];
+    for (int side = 0; side < 2; ++side) {
+        glast[side] = p.group_count[side] - 1;
+        slast[side] = p.groups[side][glast[side]].start;
+        s_min = std::min(s_min, slast[side]);
+    }
+    if (slast[0] > p.tile_level || slast[1] > p.tile_level || s_min == 0) {
+        return e;
+    }
+    const uint64_t tiles = 1ull << p.tile_level;
+    const uint64_t span = 1ull << (p.tile_level - s_min); // tiles per coarsest root
+    if (tiles < (uint64_t)kTileParts * span || tiles < (uint64_t)kTileParts * 2048) {
+        return e;
+    }
+    const uint64_t step = tiles / kTileParts / span * span;
+    for (uint32_t k = 0; k + 1 < kTileParts; ++k) {
+        const uint64_t cut = step * (k + 1);
+        std::array<uint64_t, 2> at{};
+        for (int side = 0; side < 2; ++side) {
+            const uint64_t root = cut >> (p.tile_level - slast[side]);
+            at[side] = p.section_offset[side] +
+                cluster_base(p, side, glast[side], slast[side], root) / 8;
+        }
+        e.cuts.push_back(cut);
+        e.upto.push_back(at);
+    }
+    e.cuts.push_back(tiles);
+    return e;
 }
 
 // Narrowing of 64-bit host inputs before the upload (on unless the
@@ -1100,56 +1167,109 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
                 "blob download");
         }
     };
-    EarlyPart early;
-    const bool split = end == call.plan->end_offset && early_part(*call.plan, &early);
-    std::thread helper;
+    // Early pieces go down on the copy stream after the event that makes
+    // them final; a pageable blob goes through the ring on a helper thread,
+    // which takes the pieces in order from a queue.
+    EarlyPlan early;
+    if (end == call.plan->end_offset) {
+        early = early_plan(*call.plan);
+    }
+    uint64_t done[2] = {0, call.plan->section_offset[1]}; // bytes handed out, per section
+    struct Piece {
+        cudaEvent_t ev;
+        uint64_t off, len;
+    };
+    std::mutex qm;
+    std::condition_variable qcv;
+    std::vector<Piece> queue;
+    bool closed = false;
     std::atomic<int> helper_failed{0};
+    std::thread helper;
     struct Join {
         std::thread& t;
+        std::mutex& m;
+        std::condition_variable& cv;
+        bool& closed;
         ~Join() {
+            {
+                std::lock_guard<std::mutex> lock(m);
+                closed = true;
+            }
+            cv.notify_all();
             if (t.joinable()) t.join();
         }
-    } join{helper};
-    const LevelHook hook = [&](uint32_t level) {
-        if (level != early.level) {
-            return;
-        }
-        check(cudaEventRecord(w.early, w.stream), "cudaEventRecord");
-        check(cudaStreamWaitEvent(w.copy_stream, w.early, 0), "cudaStreamWaitEvent");
-        if (!stage_out) {
-            download(early.off[0], early.len[0], w.copy_stream);
-            download(early.off[1], early.len[1], w.copy_stream);
-            return;
-        }
+    } join{helper, qm, qcv, closed};
+    if (stage_out && (early.levels || !early.cuts.empty())) {
         helper = std::thread([&] {
-            try {
-                download(early.off[0], early.len[0], w.copy_stream);
-                download(early.off[1], early.len[1], w.copy_stream);
-            } catch (const CudaFail&) {
-                helper_failed.store(1);
+            size_t next = 0;
+            for (;;) {
+                Piece piece{};
+                {
+                    std::unique_lock<std::mutex> lock(qm);
+                    qcv.wait(lock, [&] { return closed || next < queue.size(); });
+                    if (next >= queue.size()) return;
+                    piece = queue[next++];
+                }
+                try {
+                    check(cudaStreamWaitEvent(w.copy_stream, piece.ev, 0), "cudaStreamWaitEvent");
+                    download(piece.off, piece.len, w.copy_stream);
+                } catch (const CudaFail&) {
+                    helper_failed.store(1);
+                    return;
+                }
             }
         });
+    }
+    auto hand_out = [&](cudaEvent_t ev, const uint64_t (&to)[2]) {
+        check(cudaEventRecord(ev, w.stream), "cudaEventRecord");
+        for (int side = 0; side < 2; ++side) {
+            const uint64_t off = side == 0 ? done[0] : done[1];
+            if (to[side] <= off) continue;
+            if (stage_out) {
+                std::lock_guard<std::mutex> lock(qm);
+                queue.push_back(Piece{ev, off, to[side] - off});
+            } else {
+                check(cudaStreamWaitEvent(w.copy_stream, ev, 0), "cudaStreamWaitEvent");
+                download(off, to[side] - off, w.copy_stream);
+            }
+            done[side] = to[side];
+        }
+        qcv.notify_all();
+    };
+    const LevelHook level_hook = [&](uint32_t level) {
+        if (level == early.level) {
+            hand_out(w.early, early.first);
+        }
+    };
+    TileParts parts;
+    parts.cuts = early.cuts;
+    parts.after_part = [&](uint32_t k) {
+        if (k < early.upto.size()) {
+            const uint64_t to[2] = {early.upto[k][0], early.upto[k][1]};
+            hand_out(w.parts[k], to);
+        }
     };
     rc = run(w, call, w.stream, w.input, device_width, w.blob, device_seconds, err, err_len,
-        split ? &hook : nullptr);
+        early.levels ? &level_hook : nullptr, early.cuts.empty() ? nullptr : &parts);
+    {
+        std::lock_guard<std::mutex> lock(qm);
+        closed = true;
+    }
+    qcv.notify_all();
     if (helper.joinable()) {
         helper.join();
     }
-    if (split) {
-        check(cudaStreamSynchronize(w.copy_stream), "cudaStreamSynchronize");
-    }
+    check(cudaStreamSynchronize(w.copy_stream), "cudaStreamSynchronize");
     if (rc != kOk) {
         return rc;
     }
     if (helper_failed.load()) {
         throw CudaFail{cudaErrorUnknown, "staged blob download"};
     }
-    if (split) {
-        download(early.len[0], early.off[1] - early.len[0], w.stream);
-        download(early.off[1] + early.len[1], end - early.off[1] - early.len[1], w.stream);
-    } else {
-        download(0, end, w.stream);
-    }
+    // the rest: the tail of each section and whatever follows the output
+    // section (the separate middle section)
+    download(done[0], call.plan->section_offset[1] - done[0], w.stream);
+    download(done[1], end - done[1], w.stream);
     check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
     return kOk;
 }

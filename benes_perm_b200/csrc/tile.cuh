@@ -537,10 +537,11 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
 template <typename T>
 __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __restrict__ plan,
     const T* __restrict__ src, uint32_t* __restrict__ blob, uint32_t* status, uint32_t slots,
-    uint32_t pairs) {
+    uint32_t pairs, uint32_t part_first) {
     extern __shared__ __align__(16) unsigned char smem[];
-    // a sharded call encodes only its own tiles (level_nodes)
-    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo;
+    // a sharded call encodes only its own tiles (level_nodes); a launch may
+    // cover a part of them, from tile part_first on
+    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo + part_first;
     tile_body<T>(plan, src, blob, status, slots, pairs, first + blockIdx.x, smem);
 }
 
@@ -550,9 +551,9 @@ __global__ void __launch_bounds__(kTileThreads, 2) tile_encode(const Plan* __res
 template <typename T>
 __global__ void __launch_bounds__(2 * kTileThreads, 1) tile_encode_wide(
     const Plan* __restrict__ plan, const T* __restrict__ src, uint32_t* __restrict__ blob,
-    uint32_t* status, uint32_t slots, uint32_t pairs) {
+    uint32_t* status, uint32_t slots, uint32_t pairs, uint32_t part_first) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo;
+    const uint32_t first = (uint32_t)level_nodes(*plan, plan->tile_level).lo + part_first;
     tile_body<T>(plan, src, blob, status, slots, pairs, first + blockIdx.x, smem);
 }
 

@@ -154,14 +154,19 @@ def test_host_path_early_download(gpu, oracle):
     # the staging ring on a helper thread into a pageable one.  Both must
     # equal the device-resident path, and one format the oracle.
     import torch
-    n = (1 << 23) + 12345
     cases = [dict(middle_group_log2=4, middle_placement=0),
              dict(middle_group_log2=5, middle_placement=2),
              dict(middle_group_log2=4, middle_placement=1, input_clusters=[4, 7, 9],
                   output_clusters=[10, 10]),
              dict(middle_group_log2=5, middle_placement=0, input_clusters=[4, 7, 8],
                   output_clusters=[10, 9])]
+    # 2^27 + 12345 entries: 16384 or 32768 tiles, launched in 8 parts, the blob's
+    # finished clusters downloaded after each part
+    cases.append(dict(middle_group_log2=5, middle_placement=2, n=(1 << 27) + 12345))
+    cases.append(dict(middle_group_log2=4, middle_placement=0, n=(1 << 27) + 12345))
     for i, kw in enumerate(cases):
+        kw = dict(kw)
+        n = kw.pop("n", (1 << 23) + 12345)
         dtype = np.uint64 if i % 2 else np.uint32
         perm = gpu.fill_permutation(gpu.PermutationKind(i % 2), 0xE4 + i, n, dtype)
         fmt = b200_format(gpu, kw)

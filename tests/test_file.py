@@ -11,6 +11,8 @@ work, so they are tested on the CPU too.
 import numpy as np
 import pytest
 
+from helpers import oracle_format
+
 
 def _write(path, values, dtype):
     np.asarray(values).astype(dtype).tofile(path)
@@ -60,9 +62,9 @@ def test_file_matches_oracle(gpu, oracle, tmp_path, n, width):
     (5_000_011, 4, 4, 0),
     ((1 << 22), 4, 5, 1),
 ])
-def test_file_matches_memory_encode(gpu, tmp_path, n, width, m, placement):
+def test_file_matches_memory_encode(gpu, oracle, tmp_path, n, width, m, placement):
     """Multi-chunk files: the streamed upload and download give the bytes of
-    the in-memory encode of the same values."""
+    the in-memory encode of the same values, and (one size) of the oracle."""
     dtype = np.uint32 if width == 4 else np.uint64
     perm = gpu.fill_permutation(gpu.PermutationKind.uniform, n, n, dtype)
     src = tmp_path / "in.bin"
@@ -74,6 +76,9 @@ def test_file_matches_memory_encode(gpu, tmp_path, n, width, m, placement):
     gpu.compress_file(src, out, width, opts)
     assert out.read_bytes() == gpu.compress(perm, opts)
     assert gpu.last_device_seconds() > 0
+    if n == 5_000_011:
+        assert out.read_bytes() == oracle.compress(
+            perm, oracle_format(dict(middle_group_log2=m, middle_placement=placement)))
 
 
 @pytest.mark.gpu

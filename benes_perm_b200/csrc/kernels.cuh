@@ -58,7 +58,7 @@ constexpr int kInverseItems = BPB200_INVERSE_ITEMS; // slots per thread in level
 #define BPB200_UNION_MIN_BLOCKS 4
 #endif
 constexpr int kUnionItems = BPB200_UNION_ITEMS; // output pairs per thread in level_union
-// level_finalize shape: pair-nodes per thread (2, 4 or 8; 32 / items lanes
+// level_finalize shape: pair-nodes per thread (1, 2, 4 or 8; 32 / items lanes
 // assemble one colour word) and the minimum resident blocks of 256 per SM.
 // 2 pair-nodes at 8 blocks measured fastest on B200 at 2^30 uniform entries
 // (finalize 115 ms per compress; 2 at 6 blocks: 120; 4 at 6 blocks: 144;
@@ -71,8 +71,8 @@ constexpr int kUnionItems = BPB200_UNION_ITEMS; // output pairs per thread in le
 #define BPB200_FINAL_MIN_BLOCKS 8
 #endif
 constexpr int kResolveItems = BPB200_RESOLVE_ITEMS;
-static_assert(kResolveItems == 2 || kResolveItems == 4 || kResolveItems == 8,
-    "level_finalize assembles colour words from 2, 4 or 8 bits per lane");
+static_assert(kResolveItems == 1 || kResolveItems == 2 || kResolveItems == 4 ||
+    kResolveItems == 8, "level_finalize assembles colour words from 1, 2, 4 or 8 bits per lane");
 
 struct TileShape {
     uint32_t slots;   // padded entry slots needed at the deepest level

@@ -17,6 +17,7 @@
 
 #include <cuda_runtime.h>
 #include <dlfcn.h>
+#include <immintrin.h>
 
 #include <algorithm>
 #include <array>
@@ -1060,6 +1061,51 @@ EarlyPlan early_plan(const Plan& p) {
     return e;
 }
 
+// out[i] = (uint32_t)in[i] for i < n; true when some value needs more than
+// 32 bits.  With AVX2 the stores bypass the cache (the pinned chunk is read
+// next by the copy engine, not by this thread), which saves the read for
+// ownership of every destination line.
+__attribute__((target("avx2"))) bool narrow_values_avx2(const uint64_t* in, uint32_t* out,
+    uint64_t n) {
+    uint64_t i = 0;
+    __m256i high = _mm256_setzero_si256();
+    const __m256i pick = _mm256_setr_epi32(0, 2, 4, 6, 1, 3, 5, 7);
+    if (((uintptr_t)out & 31) == 0) {
+        for (; i + 8 <= n; i += 8) {
+            const __m256i a = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(in + i));
+            const __m256i b = _mm256_loadu_si256(reinterpret_cast<const __m256i*>(in + i + 4));
+            high = _mm256_or_si256(high, _mm256_or_si256(a, b));
+            // low halves of a's four values, then of b's
+            const __m256i la = _mm256_permutevar8x32_epi32(a, pick);
+            const __m256i lb = _mm256_permutevar8x32_epi32(b, pick);
+            _mm256_stream_si256(reinterpret_cast<__m256i*>(out + i),
+                _mm256_permute2x128_si256(la, lb, 0x20));
+        }
+        _mm_sfence();
+    }
+    alignas(32) uint64_t lanes[4];
+    _mm256_store_si256(reinterpret_cast<__m256i*>(lanes), high);
+    uint64_t wide = lanes[0] | lanes[1] | lanes[2] | lanes[3];
+    for (; i < n; ++i) {
+        wide |= in[i];
+        out[i] = (uint32_t)in[i];
+    }
+    return (wide >> 32) != 0;
+}
+
+bool narrow_values(const uint64_t* in, uint32_t* out, uint64_t n) {
+    static const bool avx2 = __builtin_cpu_supports("avx2") != 0;
+    if (avx2) {
+        return narrow_values_avx2(in, out, n);
+    }
+    uint64_t wide = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        wide |= in[i];
+        out[i] = (uint32_t)in[i];
+    }
+    return (wide >> 32) != 0;
+}
+
 // Narrowing of 64-bit host inputs before the upload (on unless the
 // environment sets BPB200_NARROW_UPLOAD=0), with up to 16 host threads.
 bool narrow_upload_enabled() {
@@ -1114,15 +1160,9 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
         std::atomic<uint64_t> wide{0};
         upload_staged(
             [src, &wide](unsigned char* dst, uint64_t len, uint64_t off) {
-                uint32_t* out = reinterpret_cast<uint32_t*>(dst);
-                const uint64_t* in = src + off / 4;
-                const uint64_t n = len / 4;
-                uint64_t high = 0;
-                for (uint64_t i = 0; i < n; ++i) {
-                    high |= in[i];
-                    out[i] = (uint32_t)in[i];
+                if (narrow_values(src + off / 4, reinterpret_cast<uint32_t*>(dst), len / 4)) {
+                    wide.fetch_or(1);
                 }
-                if (high >> 32) wide.fetch_or(1);
                 return true;
             },
             count * 4, (unsigned char*)w.input, *ring->r, w.stream, narrow_threads());

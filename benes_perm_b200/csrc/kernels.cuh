@@ -47,6 +47,11 @@ constexpr uint32_t kTileThreads = 512;
 #endif
 static_assert(BPB200_INVERSE_ITEMS % 4 == 0, "level_inverse initialises owners 4 at a time");
 constexpr int kInverseItems = BPB200_INVERSE_ITEMS; // slots per thread in level_inverse
+// Walk owners: one word per pair-node (the stamp of its even vertex; 1) or
+// one per slot (0).
+#ifndef BPB200_PAIR_OWNERS
+#define BPB200_PAIR_OWNERS 1
+#endif
 // level_union shape: 2 output pairs per thread with at most 64 registers (4
 // blocks of 256 per SM) measured fastest on B200 at 2^30 uniform entries
 // (union kernels 253 ms per compress; 4 pairs at 100 registers: 304 ms;
@@ -122,6 +127,7 @@ __device__ __forceinline__ void level_inverse_run(Grid grid, const Plan* __restr
         uint32_t j = (uint32_t)(e0 / cap);
         uint32_t i = (uint32_t)(e0 - (uint64_t)j * cap);
         uint32_t s = size_at(lv, level, j);
+#if !BPB200_PAIR_OWNERS
         // every slot starts unowned for the orbit walks
         if (e0 + kInverseItems <= total) {
             uint4* o = reinterpret_cast<uint4*>(owner + e0);
@@ -132,14 +138,18 @@ __device__ __forceinline__ void level_inverse_run(Grid grid, const Plan* __restr
         } else {
             for (uint64_t e = e0; e < total; ++e) owner[e] = ~0u;
         }
+#endif
 #pragma unroll
         for (int q = 0; q < kInverseItems; ++q) {
             if (e0 + q < total && i < s) {
                 // every pair-node starts as its own root, whatever its values:
-                // a stale word could point outside the array
+                // a stale word could point outside the array; and unowned
                 if ((i & 1u) == 0) {
                     const uint32_t id = j * pcap + (i >> 1);
                     uf[id] = id << 1;
+#if BPB200_PAIR_OWNERS
+                    owner[id] = ~0u;
+#endif
                 }
                 const uint64_t val = (uint64_t)v[q];
                 if (val >= s) {
@@ -489,14 +499,18 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
                     child_inv[lb + k] = to_left;
                     child_inv[rb + k] = to_right;
                 }
+#if !BPB200_PAIR_OWNERS
                 if (child_owner != nullptr) {
                     child_owner[lb + k] = ~0u;
                     child_owner[rb + k] = ~0u;
                 }
+#endif
             } else if (k == half && (s & 1u) != 0) {
                 const uint32_t u = inv[node + s - 1];
                 if (child_inv != nullptr) child_inv[lb + half] = u < s ? u >> 1 : ~0u;
+#if !BPB200_PAIR_OWNERS
                 if (child_owner != nullptr) child_owner[lb + half] = ~0u;
+#endif
             }
             // children's pair-nodes start as their own roots: left child of
             // s - s/2 entries, right of s/2; pair-node k/2 for even k
@@ -510,6 +524,13 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
                     child_uf[id] = id << 1;
                 }
             }
+#if BPB200_PAIR_OWNERS
+            // children's walk owners, one per pair-node, start unset
+            if (child_owner != nullptr && (k & 1u) == 0) {
+                if (k < s - half) child_owner[2 * j * cpcap + (k >> 1)] = ~0u;
+                if (k < half) child_owner[(2 * j + 1) * cpcap + (k >> 1)] = ~0u;
+            }
+#endif
         }
         const unsigned word = __ballot_sync(0xffffffffu, y);
         if ((threadIdx.x & 31) == 0) {

@@ -76,6 +76,9 @@ constexpr uint64_t kWalkMaxNode = 1ull << BPB200_WALK_MAX_LOG2; // larger: union
 static_assert(BPB200_RULER_LOG2 >= 2 && BPB200_RULER_LOG2 <= 8, "ruler density out of range");
 static_assert(BPB200_WALK_MAX_LOG2 >= 13 && BPB200_WALK_MAX_LOG2 <= 28, "walk limit out of range");
 constexpr uint32_t kUnset = 0xffffffffu;     // owner of a vertex no walk reached
+// owner word of even vertex v of a node: own_base + (v >> kOwnShift), the
+// base being the node's first pair-node (pair-indexed owners) or slot
+constexpr uint32_t kOwnShift = BPB200_PAIR_OWNERS ? 1u : 0u;
 constexpr uint32_t kColourTag = 0x80000000u; // owner value carrying a colour directly
 constexpr uint32_t kNoRuler = 0xffffffffu;   // bucket whose hashed slot is padding
 
@@ -169,7 +172,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
     uint32_t next_free = 0, hi = 0; // current chunk, warp-uniform
     bool exhausted = false;
     bool active = false;
-    uint32_t r = 0, base = 0, s = 0, cur = 0, ma = 0, mb = 0, steps = 0;
+    uint32_t r = 0, base = 0, own = 0, s = 0, cur = 0, ma = 0, mb = 0, steps = 0;
     bool odd = false;
     for (;;) {
         const unsigned idle = __ballot_sync(0xffffffffu, !active);
@@ -198,6 +201,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
                     state[r] = make_uint4(kNoRuler, 0, 0, 0);
                 } else {
                     base = j * cap;
+                    own = BPB200_PAIR_OWNERS ? j * (uint32_t)lv.pcap : base;
                     odd = (s & 1u) != 0;
                     const NodeView<T> nv{vals + base, inv + base, s, odd};
                     cur = v0;
@@ -225,7 +229,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
                 next = (base + w) >> kRulerLog2;
                 end = true;
             } else {
-                if (w < s && (w & 1u) == 0) owner[base + w] = r;
+                if (w < s && (w & 1u) == 0) owner[own + (w >> kOwnShift)] = r;
                 ma = min(ma, nv.key(w));
                 mb = min(mb, nv.key(w ^ 1u));
                 cur = w;
@@ -275,8 +279,9 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
             continue;
         }
         const uint32_t base = j * cap;
+        const uint32_t own = BPB200_PAIR_OWNERS ? j * pcap : base;
         const uint32_t v = 2 * k;
-        if (is_ruler_slot(base + v) || owner[base + v] != kUnset) {
+        if (is_ruler_slot(base + v) || owner[own + (v >> kOwnShift)] != kUnset) {
             continue;
         }
         const NodeView<T> nv{vals + base, inv + base, s, (s & 1u) != 0};
@@ -312,7 +317,7 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
         const uint32_t colour = kColourTag | (ma > mb ? 1u : 0u);
         cur = v;
         do {
-            if (cur < s) owner[base + cur] = colour;
+            if (cur < s && (cur & 1u) == 0) owner[own + (cur >> kOwnShift)] = colour;
             cur = nv.f(cur);
         } while (cur != v);
     }
@@ -736,7 +741,8 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
             for (int q = 0; q < kResolveItems; ++q) {
                 if (!(live & (1u << q))) continue;
                 const uint32_t slot = jj[q] * cap + 2 * kk[q];
-                id[q] = is_ruler_slot(slot) ? slot >> kRulerLog2 : owner[slot];
+                id[q] = is_ruler_slot(slot) ? slot >> kRulerLog2
+                    : owner[BPB200_PAIR_OWNERS ? jj[q] * pcap + kk[q] : slot];
             }
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {

@@ -88,7 +88,7 @@ struct Workspace {
     uint32_t* uf = nullptr;
     uint32_t* xbits = nullptr;
     uint32_t* ybits = nullptr;
-    uint32_t* owner = nullptr;             // ruler id stamped on each walked vertex
+    uint32_t* owner = nullptr;             // ruler id stamped on each walked even vertex, per pair-node
     uint4* state[2] = {nullptr, nullptr};  // ruler states; [1] holds the super-ruler states
     uint32_t* super_of = nullptr;          // super-ruler (or stamped colour) of each ruler
     uint32_t* control = nullptr;           // per-level control words (walk.cuh)
@@ -207,7 +207,7 @@ void ensure_scratch(Workspace& w, const Plan& p) {
     check(cudaMalloc(&w.uf, pairs * 4), "cudaMalloc(union-find)");
     check(cudaMalloc(&w.xbits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(colour bits)");
     check(cudaMalloc(&w.ybits, ((pairs + 31) / 32 + 1) * 4), "cudaMalloc(output bits)");
-    check(cudaMalloc(&w.owner, slots * 4), "cudaMalloc(owners)");
+    check(cudaMalloc(&w.owner, pairs * 4), "cudaMalloc(owners)"); // one per pair-node
     const uint64_t buckets = (slots >> kRulerLog2) + 1;
     check(cudaMalloc(&w.state[0], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
     check(cudaMalloc(&w.state[1], buckets * sizeof(uint4)), "cudaMalloc(ruler state)");
@@ -1568,7 +1568,7 @@ constexpr size_t kOffYbits = kOffXbits + up256((kPairs / 32 + 1) * 4);
 constexpr size_t kOffAddr0 = kOffYbits + up256((kPairs / 32 + 1) * 4);
 constexpr size_t kOffAddr1 = kOffAddr0 + up256(kNodes * sizeof(NodeAddress));
 constexpr size_t kOffOwner = kOffAddr1 + up256(kNodes * sizeof(NodeAddress));
-constexpr size_t kOffState0 = kOffOwner + up256(kSlots * 4);
+constexpr size_t kOffState0 = kOffOwner + up256(kPairs * 4);
 constexpr size_t kOffState1 = kOffState0 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffSuper = kOffState1 + up256(((kSlots >> kRulerLog2) + 1) * sizeof(uint4));
 constexpr size_t kOffControl = kOffSuper + up256(((kSlots >> kRulerLog2) + 1) * 4);

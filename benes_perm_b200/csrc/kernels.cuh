@@ -45,13 +45,7 @@ constexpr uint32_t kTileThreads = 512;
 #ifndef BPB200_INVERSE_ITEMS
 #define BPB200_INVERSE_ITEMS 4
 #endif
-static_assert(BPB200_INVERSE_ITEMS % 4 == 0, "level_inverse initialises owners 4 at a time");
 constexpr int kInverseItems = BPB200_INVERSE_ITEMS; // slots per thread in level_inverse
-// Walk owners: one word per pair-node (the stamp of its even vertex; 1) or
-// one per slot (0).
-#ifndef BPB200_PAIR_OWNERS
-#define BPB200_PAIR_OWNERS 1
-#endif
 // level_union shape: 2 output pairs per thread with at most 64 registers (4
 // blocks of 256 per SM) measured fastest on B200 at 2^30 uniform entries
 // (union kernels 253 ms per compress; 4 pairs at 100 registers: 304 ms;
@@ -127,18 +121,6 @@ __device__ __forceinline__ void level_inverse_run(Grid grid, const Plan* __restr
         uint32_t j = (uint32_t)(e0 / cap);
         uint32_t i = (uint32_t)(e0 - (uint64_t)j * cap);
         uint32_t s = size_at(lv, level, j);
-#if !BPB200_PAIR_OWNERS
-        // every slot starts unowned for the orbit walks
-        if (e0 + kInverseItems <= total) {
-            uint4* o = reinterpret_cast<uint4*>(owner + e0);
-#pragma unroll
-            for (int q = 0; q < kInverseItems / 4; ++q) {
-                o[q] = make_uint4(~0u, ~0u, ~0u, ~0u);
-            }
-        } else {
-            for (uint64_t e = e0; e < total; ++e) owner[e] = ~0u;
-        }
-#endif
 #pragma unroll
         for (int q = 0; q < kInverseItems; ++q) {
             if (e0 + q < total && i < s) {
@@ -147,9 +129,7 @@ __device__ __forceinline__ void level_inverse_run(Grid grid, const Plan* __restr
                 if ((i & 1u) == 0) {
                     const uint32_t id = j * pcap + (i >> 1);
                     uf[id] = id << 1;
-#if BPB200_PAIR_OWNERS
                     owner[id] = ~0u;
-#endif
                 }
                 const uint64_t val = (uint64_t)v[q];
                 if (val >= s) {
@@ -450,11 +430,10 @@ __global__ void level_descriptors(const Plan* __restrict__ plan, uint32_t level,
 // and an odd node's tail output s - 1, whose input is coloured 0, gives
 // left_inv[s / 2] = inv[s - 1] >> 1.  The pass reads inv sequentially and
 // one colour bit per output pair, and writes the children's inverse
-// sequentially.  It also resets the children's walk owners (every slot: the
-// walks read only even ones, but writing every other word turns each
-// 32-byte sector into a read-modify-write, measured 3.7 ms slower per
-// 2^30 compress) and pair-node union-find roots (`child_owner` / `child_uf`,
-// may be null), the state the next level's colouring starts from.  A value out of range (only
+// sequentially.  It also resets the children's walk owners (one word per
+// pair-node: the stamp of its even vertex, the only one the walks read) and
+// pair-node union-find roots (`child_owner` / `child_uf`, may be null), the
+// state the next level's colouring starts from.  A value out of range (only
 // possible when the input was not a permutation, which level 0 reports)
 // leaves 0xffffffff, which every user range-checks.
 __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restrict__ plan,
@@ -499,18 +478,9 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
                     child_inv[lb + k] = to_left;
                     child_inv[rb + k] = to_right;
                 }
-#if !BPB200_PAIR_OWNERS
-                if (child_owner != nullptr) {
-                    child_owner[lb + k] = ~0u;
-                    child_owner[rb + k] = ~0u;
-                }
-#endif
             } else if (k == half && (s & 1u) != 0) {
                 const uint32_t u = inv[node + s - 1];
                 if (child_inv != nullptr) child_inv[lb + half] = u < s ? u >> 1 : ~0u;
-#if !BPB200_PAIR_OWNERS
-                if (child_owner != nullptr) child_owner[lb + half] = ~0u;
-#endif
             }
             // children's pair-nodes start as their own roots: left child of
             // s - s/2 entries, right of s/2; pair-node k/2 for even k
@@ -524,13 +494,11 @@ __device__ __forceinline__ void level_outputs_run(Grid grid, const Plan* __restr
                     child_uf[id] = id << 1;
                 }
             }
-#if BPB200_PAIR_OWNERS
             // children's walk owners, one per pair-node, start unset
             if (child_owner != nullptr && (k & 1u) == 0) {
                 if (k < s - half) child_owner[2 * j * cpcap + (k >> 1)] = ~0u;
                 if (k < half) child_owner[(2 * j + 1) * cpcap + (k >> 1)] = ~0u;
             }
-#endif
         }
         const unsigned word = __ballot_sync(0xffffffffu, y);
         if ((threadIdx.x & 31) == 0) {

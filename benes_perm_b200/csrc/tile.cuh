@@ -45,13 +45,6 @@ __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pa
     return o;
 }
 
-// Unions per thread in the tile's union phase, their finds in lockstep (1:
-// one union at a time).
-#ifndef BPB200_TILE_UNION_PAIRS
-#define BPB200_TILE_UNION_PAIRS 1
-#endif
-constexpr int kTileUnions = BPB200_TILE_UNION_PAIRS;
-
 // Tile input through one bulk asynchronous copy (1) or batched plain loads (0).
 #ifndef BPB200_TILE_BULK_LOAD
 #define BPB200_TILE_BULK_LOAD 0
@@ -259,35 +252,6 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             // node's few roots (with 16 nodes of 256 pair-nodes, node-major
             // order ran all 256 unions of a node at once; tile time at 2^30
             // entries 157 -> 145 ms).
-#if BPB200_TILE_UNION_PAIRS > 1
-            // kTileUnions unions per thread with their finds in lockstep
-            for (uint32_t idx0 = tid; idx0 < nodes * pcap; idx0 += kTileUnions * blockDim.x) {
-                uint32_t a[kTileUnions], b[kTileUnions], rel[kTileUnions];
-                uint32_t pending = 0;
-#pragma unroll
-                for (int q = 0; q < kTileUnions; ++q) {
-                    const uint32_t idx = idx0 + q * blockDim.x;
-                    a[q] = b[q] = rel[q] = 0;
-                    if (idx >= nodes * pcap) continue;
-                    const uint32_t path = idx & (nodes - 1);
-                    const uint32_t k = idx >> t;
-                    const uint32_t s = size_at(lv, level, first + path);
-                    if (k >= s / 2 || !internal_node(path, s)) continue;
-                    const uint32_t u = inv[path * cap + 2 * k];
-                    const uint32_t w = inv[path * cap + 2 * k + 1];
-                    if (u >= s || w >= s) {
-                        atomicOr(status, kErrNotPermutation);
-                        continue;
-                    }
-                    const uint32_t base = path * pcap;
-                    a[q] = base + (u >> 1);
-                    b[q] = base + (w >> 1);
-                    rel[q] = 1u ^ (u & 1u) ^ (w & 1u);
-                    pending |= 1u << q;
-                }
-                uf_union_many<kTileUnions>(uf, a, b, rel, pending, status);
-            }
-#else
             for (uint32_t idx = tid; idx < nodes * pcap; idx += blockDim.x) {
                 const uint32_t path = idx & (nodes - 1);
                 const uint32_t k = idx >> t;
@@ -304,7 +268,6 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 const uint32_t base = path * pcap;
                 uf_union(uf, base + (u >> 1), base + (w >> 1), 1u ^ (u & 1u) ^ (w & 1u), status);
             }
-#endif
             __syncthreads();
             // C: orient odd nodes so the unpaired tail gets colour 0
             for (uint32_t path = tid; path < nodes; path += blockDim.x) {

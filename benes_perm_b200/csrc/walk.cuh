@@ -76,9 +76,9 @@ constexpr uint64_t kWalkMaxNode = 1ull << BPB200_WALK_MAX_LOG2; // larger: union
 static_assert(BPB200_RULER_LOG2 >= 2 && BPB200_RULER_LOG2 <= 8, "ruler density out of range");
 static_assert(BPB200_WALK_MAX_LOG2 >= 13 && BPB200_WALK_MAX_LOG2 <= 28, "walk limit out of range");
 constexpr uint32_t kUnset = 0xffffffffu;     // owner of a vertex no walk reached
-// owner word of even vertex v of a node: own_base + (v >> kOwnShift), the
-// base being the node's first pair-node (pair-indexed owners) or slot
-constexpr uint32_t kOwnShift = BPB200_PAIR_OWNERS ? 1u : 0u;
+// Walk owners are one word per pair-node: owner[j * pcap + k] is the stamp
+// of even vertex 2k of node j (the finalize reads only even vertices), half
+// the footprint of a word per slot, which keeps more of a node in L2.
 constexpr uint32_t kColourTag = 0x80000000u; // owner value carrying a colour directly
 constexpr uint32_t kNoRuler = 0xffffffffu;   // bucket whose hashed slot is padding
 
@@ -159,7 +159,7 @@ struct NodeView {
 // the next ruler of the chunk as soon as its current walk ends, so walk
 // lengths (geometric, mean 2^kRulerLog2) do not leave lanes idle behind the
 // longest walk.  state[r] = {next ruler, min key, min mirror key, 0};
-// owner[slot] = r for every real vertex the walk passes.
+// owner[pair-node] = r for every real even vertex the walk passes.
 template <typename T>
 __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     const T* __restrict__ vals, const uint32_t* __restrict__ inv, uint32_t* __restrict__ owner,
@@ -201,7 +201,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
                     state[r] = make_uint4(kNoRuler, 0, 0, 0);
                 } else {
                     base = j * cap;
-                    own = BPB200_PAIR_OWNERS ? j * (uint32_t)lv.pcap : base;
+                    own = j * (uint32_t)lv.pcap;
                     odd = (s & 1u) != 0;
                     const NodeView<T> nv{vals + base, inv + base, s, odd};
                     cur = v0;
@@ -229,7 +229,7 @@ __device__ __forceinline__ void level_walk_run(Grid grid, const Plan* __restrict
                 next = (base + w) >> kRulerLog2;
                 end = true;
             } else {
-                if (w < s && (w & 1u) == 0) owner[own + (w >> kOwnShift)] = r;
+                if (w < s && (w & 1u) == 0) owner[own + (w >> 1)] = r;
                 ma = min(ma, nv.key(w));
                 mb = min(mb, nv.key(w ^ 1u));
                 cur = w;
@@ -279,9 +279,9 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
             continue;
         }
         const uint32_t base = j * cap;
-        const uint32_t own = BPB200_PAIR_OWNERS ? j * pcap : base;
+        const uint32_t own = j * pcap;
         const uint32_t v = 2 * k;
-        if (is_ruler_slot(base + v) || owner[own + (v >> kOwnShift)] != kUnset) {
+        if (is_ruler_slot(base + v) || owner[own + k] != kUnset) {
             continue;
         }
         const NodeView<T> nv{vals + base, inv + base, s, (s & 1u) != 0};
@@ -317,7 +317,7 @@ __device__ __forceinline__ void level_walk_short_run(Grid grid, const Plan* __re
         const uint32_t colour = kColourTag | (ma > mb ? 1u : 0u);
         cur = v;
         do {
-            if (cur < s && (cur & 1u) == 0) owner[own + (cur >> kOwnShift)] = colour;
+            if (cur < s && (cur & 1u) == 0) owner[own + (cur >> 1)] = colour;
             cur = nv.f(cur);
         } while (cur != v);
     }
@@ -741,8 +741,7 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
             for (int q = 0; q < kResolveItems; ++q) {
                 if (!(live & (1u << q))) continue;
                 const uint32_t slot = jj[q] * cap + 2 * kk[q];
-                id[q] = is_ruler_slot(slot) ? slot >> kRulerLog2
-                    : owner[BPB200_PAIR_OWNERS ? jj[q] * pcap + kk[q] : slot];
+                id[q] = is_ruler_slot(slot) ? slot >> kRulerLog2 : owner[jj[q] * pcap + kk[q]];
             }
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {

@@ -61,6 +61,12 @@ namespace bpb200 {
 #ifndef BPB200_FINAL_STRIDE_LOG2
 #define BPB200_FINAL_STRIDE_LOG2 26
 #endif
+// Union-find levels: level_finalize writes each pair-node's root back (1),
+// measured on B200 at 2^30 uniform entries: finalize 105.0 ms per compress
+// against 106.2 without.
+#ifndef BPB200_RESOLVE_WRITEBACK
+#define BPB200_RESOLVE_WRITEBACK 1
+#endif
 
 
 constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
@@ -731,6 +737,13 @@ __device__ __forceinline__ void level_finalize_run(Grid grid, const Plan* __rest
 #pragma unroll
             for (int q = 0; q < kResolveItems; ++q) {
                 if (live & (1u << q)) c[q] = f[q].bit ^ (uf[f[q].root] & 1u);
+#if BPB200_RESOLVE_WRITEBACK
+                // point the pair-node at its root (a true fact), so the
+                // finds of the pair-nodes below it end one step later
+                if ((live & (1u << q)) && f[q].root != x[q]) {
+                    uf[x[q]] = (f[q].root << 1) | f[q].bit;
+                }
+#endif
             }
         } else {
             // ruler id (or direct colour) of vertex 2k: every even vertex is

@@ -19,9 +19,9 @@
 // 2^kRulerLog2 slots (at a hashed position) is a ruler.  A ruler walks its
 // orbit up to the next ruler, stamping each even vertex it passes with its
 // id and keeping the minimum key of the segment and of the segment's
-// mirror.  Only even vertices are stamped: the colour of pair-node k is
-// the colour of vertex 2k, and halving the stamps halves the walk's
-// random writes.
+// mirror.  Only even vertices are stamped, into one owner word per
+// pair-node: the colour of pair-node k is the colour of vertex 2k, and
+// halving the stamps halves the walk's random writes and its owner array.
 // Pointer jumping over rulers (stopping after the first round that changes
 // nothing, which implies convergence on cycles) turns segment minima into
 // orbit minima.  No atomics, no shared roots: every step is two independent

@@ -61,7 +61,8 @@ int bpb200_encoded_size(uint64_t count, const bpb200_format* format,
  * time, the value the reference stores with set_last_device_seconds.
  * Errors: INVALID_ARGUMENT "input must contain every value from zero through
  * size minus one" for a non-permutation, exactly like validate_permutation
- * (src/benes.cpp:152-173). */
+ * (src/benes.cpp:152-173).  Parts of the blob are copied into `blob` while
+ * the encode still runs, so after an error its contents are unspecified. */
 int bpb200_compress(const void* entries, uint64_t count, uint32_t entry_bytes,
     const bpb200_format* format, uint8_t* blob, uint64_t blob_len,
     double* device_seconds, char* err, size_t err_len);

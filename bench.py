@@ -759,20 +759,27 @@ def serving_run(args):
         got = [hashlib.sha256(b).hexdigest()[:32] for b in blobs]
         return t_serve, np.sort(np.array(latencies)), got, launches
 
-    # capacity: every request submitted at once (offered load above capacity)
-    t_serve, lat, got, launches = serve(None)
+    # capacity: every request submitted at once (offered load above capacity),
+    # three runs on the warm server; the median run is reported (host-side
+    # staging makes single runs vary with the load on the shared host)
+    runs = [serve(None) for _ in range(3)]
+    capacity_rates = [total / r[0] for r in runs]
+    t_serve, lat, got, launches = sorted(runs, key=lambda r: r[0])[1]
+    got_all = [r[2] for r in runs]
     # latency under the stated offered load
     rate = 1.5 * len(perms) / t_plain                    # offered load, requests/s
     arrivals = np.cumsum(rng.exponential(1.0 / rate, len(perms)))
     t_paced, lat_paced, got_paced, _ = serve(arrivals)
     server.close()
-    identical = got == plain and got_paced == plain
-    ref_match = None if want is None else (plain == want and got == want and got_paced == want)
+    identical = all(g == plain for g in got_all) and got_paced == plain
+    ref_match = None if want is None else (
+        plain == want and all(g == want for g in got_all) and got_paced == want)
     return {
         "metric": "entries/s on the mixed-size serving stream (serving loop vs plain per-request)",
         "value": total / t_serve, "unit": UNIT, "n_gpus": 1, "higher_is_better": True,
         "plain_per_request": plain_rate, "ratio_vs_plain": (total / t_serve) / plain_rate,
-        "capacity": {"note": "all requests submitted at once",
+        "capacity": {"note": "all requests submitted at once; median of three runs",
+                     "runs_entries_per_s": capacity_rates,
                      "p50_latency_s": float(np.percentile(lat, 50)),
                      "p99_latency_s": float(np.percentile(lat, 99))},
         "paced": {"offered_load_requests_per_s": rate,
@@ -792,7 +799,8 @@ def serving_run(args):
                    "entries": int(total), "hbm_budget_bytes": args.hbm_budget,
                    "timing": "host wall clock (submit to blob in host memory) on one "
                              "server, warmed with 64 of the stream's requests before the "
-                             "timed runs; byte checks after the timed runs"},
+                             "timed runs; capacity: median of three runs; byte checks after "
+                             "the timed runs"},
     }
 
 

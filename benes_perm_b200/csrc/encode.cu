@@ -78,6 +78,7 @@ struct Workspace {
     cudaEvent_t start = nullptr, stop = nullptr;
     cudaEvent_t early = nullptr;        // the blob's first cluster groups are final
     cudaEvent_t parts[8] = {};          // tile parts done (progressive blob download)
+    cudaEvent_t inparts[8] = {};        // input parts on the device (host path upload)
     Plan* d_plan = nullptr;
     Plan* h_plan = nullptr;       // pinned staging for the plan upload
     uint32_t* d_status = nullptr;
@@ -132,6 +133,9 @@ struct Workspace {
         for (cudaEvent_t e : parts) {
             if (e) cudaEventDestroy(e);
         }
+        for (cudaEvent_t e : inparts) {
+            if (e) cudaEventDestroy(e);
+        }
         if (stream) cudaStreamDestroy(stream);
         if (copy_stream) cudaStreamDestroy(copy_stream);
         for (cudaEvent_t e : events) cudaEventDestroy(e);
@@ -158,6 +162,9 @@ Workspace* acquire(int device) {
     check(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&w->early, cudaEventDisableTiming), "cudaEventCreate");
     for (cudaEvent_t& e : w->parts) {
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    for (cudaEvent_t& e : w->inparts) {
         check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
     }
     check(cudaMalloc(&w->d_plan, sizeof(Plan)), "cudaMalloc(plan)");
@@ -525,10 +532,17 @@ void emission_launches(const Plan& p, uint32_t l, int side, F&& f) {
 // switch bits and the children's inverses.  `inv` holds this level's
 // inverse; `child_inv` receives the next level's (null when the next level
 // is the tile's, which builds its own in shared memory).
+// Level 0's input still arriving from the host in parts: after wait(k) the
+// stream has waited for part k, and entries [0, ends[k]) are on the device.
+struct InputParts {
+    std::vector<uint64_t> ends;
+    std::function<void(uint32_t part)> wait;
+};
+
 template <typename TV>
 void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, const Tuning& tune,
     uint32_t l, const TV* src, uint32_t* dst, uint32_t* d_blob, uint32_t* inv,
-    uint32_t* child_inv) {
+    uint32_t* child_inv, const InputParts* input = nullptr) {
     const Plan* dp = w.d_plan;
     const LevelInfo& lv = p.levels[l];
     // the whole level's extent (array layout), and this call's share of it
@@ -555,14 +569,33 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
     if (l == 0 && lv.cap > kWalkMaxNode && w.records != nullptr) {
         const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
         check(cudaMemsetAsync(w.cursor, 0, windows * 4, st), "cudaMemsetAsync(cursors)");
-        const int gb = grid_for((slots + kBucketItems - 1) / kBucketItems, kBucketThreads);
-        rec.launch(kKindPlace, [&] {
+        auto bucket = [&](uint64_t lo, uint64_t hi) {
+            const int gb = grid_for((hi - lo + kBucketItems - 1) / kBucketItems, kBucketThreads);
             level_bucket<TV><<<gb, kBucketThreads, 0, st>>>(dp, l, src, w.records, w.cursor, w.uf,
-                w.d_status);
+                w.d_status, lo, hi);
+        };
+        const uint32_t parts = input != nullptr ? (uint32_t)input->ends.size() : 0;
+        rec.launch(kKindPlace, [&] {
+            if (parts == 0) {
+                bucket(0, slots);
+            } else {
+                // each part is bucketed as soon as it is on the device, while
+                // the later parts are still being uploaded
+                uint64_t lo = 0;
+                for (uint32_t k = 0; k < parts; ++k) {
+                    input->wait(k);
+                    const uint64_t hi = std::min<uint64_t>(input->ends[k], slots);
+                    if (hi > lo) bucket(lo, hi);
+                    lo = std::max(lo, hi);
+                }
+            }
             level_place<<<grid_for(slots, kLevelThreads), kLevelThreads, 0, st>>>(dp, l,
                 w.records, w.cursor, inv, ctl + kCtlClaimPlace);
-        }, 2);
+        }, parts == 0 ? 2 : parts + 1);
     } else if (l == 0) {
+        if (input != nullptr) {
+            for (uint32_t k = 0; k < (uint32_t)input->ends.size(); ++k) input->wait(k);
+        }
         rec.launch(kKindInverse, [&] {
             level_inverse<TV><<<gs, kLevelThreads, 0, st>>>(dp, l, src, inv, w.uf, w.owner,
                 ctl + kCtlClaimInverse, w.d_status);
@@ -704,7 +737,8 @@ struct TileParts {
 template <typename T>
 void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
     const TileShape& shape, const Tuning& tune, const T* d_in, uint32_t* d_blob,
-    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr) {
+    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr,
+    const InputParts* input = nullptr) {
     const Plan* dp = w.d_plan;
     const uint32_t t0 = p.tile_level;
     if (t0 > 0) {
@@ -719,7 +753,7 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         uint32_t* dst = w.vals[l & 1];
         uint32_t* child_inv = l + 1 < t0 ? invs[(l + 1) & 1] : nullptr;
         if (l == 0) {
-            run_level<T>(w, rec, st, p, tune, l, d_in, dst, d_blob, invs[0], child_inv);
+            run_level<T>(w, rec, st, p, tune, l, d_in, dst, d_blob, invs[0], child_inv, input);
         } else {
             run_level<uint32_t>(w, rec, st, p, tune, l, cur32, dst, d_blob, invs[l & 1],
                 child_inv);
@@ -728,6 +762,10 @@ void launch_levels(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p,
         if (after_level != nullptr) {
             (*after_level)(l);
         }
+    }
+    if (t0 == 0 && input != nullptr) {
+        // the tile reads the input directly: all of it first
+        for (uint32_t k = 0; k < (uint32_t)input->ends.size(); ++k) input->wait(k);
     }
     rec.level = (int)t0;
     const uint64_t tiles = 1ull << level_nodes(p, t0).shift;
@@ -871,7 +909,8 @@ std::atomic<int> g_profiling{0};
 // Queues the whole encode on `st` and waits for it.
 int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t entry_bytes,
     uint32_t* d_blob, double* device_seconds, char* err, size_t err_len,
-    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr) {
+    const LevelHook* after_level = nullptr, const TileParts* parts = nullptr,
+    const InputParts* input = nullptr) {
     const Plan& p = *call.plan;
     ensure_scratch(w, p);
     Recorder rec;
@@ -889,10 +928,10 @@ int run(Workspace& w, Call& call, cudaStream_t st, const void* d_in, uint32_t en
     rec.launch(kKindPrologue, [&] { prologue<<<1, 128, 0, st>>>(w.d_status, d_blob, h); });
     if (entry_bytes == 4) {
         launch_levels<uint32_t>(w, rec, st, p, call.shape, call.tune, (const uint32_t*)d_in,
-            d_blob, after_level, parts);
+            d_blob, after_level, parts, input);
     } else {
         launch_levels<uint64_t>(w, rec, st, p, call.shape, call.tune, (const uint64_t*)d_in,
-            d_blob, after_level, parts);
+            d_blob, after_level, parts, input);
     }
     check(cudaEventRecord(w.stop, st), "cudaEventRecord");
     check(cudaMemcpyAsync(w.h_status, w.d_status, 4, cudaMemcpyDeviceToHost, st), "status");
@@ -1106,6 +1145,8 @@ bool narrow_values(const uint64_t* in, uint32_t* out, uint64_t n) {
     return (wide >> 32) != 0;
 }
 
+constexpr uint32_t kInputParts = 8; // host-path upload parts (see compress_host)
+
 // Narrowing of 64-bit host inputs before the upload (on unless the
 // environment sets BPB200_NARROW_UPLOAD=0), with up to 16 host threads.
 bool narrow_upload_enabled() {
@@ -1154,35 +1195,113 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
     if (narrow || stage_in || stage_out) {
         ring = std::make_unique<RingLease>(device);
     }
-    uint32_t device_width = entry_bytes;
-    if (narrow) {
-        const uint64_t* src = static_cast<const uint64_t*>(entries);
-        std::atomic<uint64_t> wide{0};
-        upload_staged(
-            [src, &wide](unsigned char* dst, uint64_t len, uint64_t off) {
-                if (narrow_values(src + off / 4, reinterpret_cast<uint32_t*>(dst), len / 4)) {
-                    wide.fetch_or(1);
-                }
-                return true;
-            },
-            count * 4, (unsigned char*)w.input, *ring->r, w.stream, narrow_threads());
-        if (wide.load() != 0) {
-            check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
-            set_error(err, err_len, "input must contain every value from zero through size minus one");
-            return kInvalidArgument;
+    const uint32_t device_width = narrow ? 4u : entry_bytes;
+    const uint64_t dev_bytes = count * device_width;
+    // Narrowing fill: true when some value needs more than 32 bits.
+    std::atomic<uint64_t> wide{0};
+    const uint64_t* src64 = static_cast<const uint64_t*>(entries);
+    const unsigned char* src8 = static_cast<const unsigned char*>(entries);
+    auto fill = [&](unsigned char* dst, uint64_t len, uint64_t off) {
+        if (narrow) {
+            if (narrow_values(src64 + off / 4, reinterpret_cast<uint32_t*>(dst), len / 4)) {
+                wide.fetch_or(1);
+            }
+        } else {
+            std::memcpy(dst, src8 + off, len);
         }
-        device_width = 4;
-    } else if (stage_in) {
-        const unsigned char* src = static_cast<const unsigned char*>(entries);
-        upload_staged(
-            [src](unsigned char* dst, uint64_t len, uint64_t off) {
-                std::memcpy(dst, src + off, len);
-                return true;
-            },
-            in_bytes, (unsigned char*)w.input, *ring->r, w.stream);
+        return true;
+    };
+    // When level 0 takes the partitioned inverse, the upload runs on the copy
+    // stream in kInputParts parts and level 0 buckets each part as soon as it
+    // is on the device (the bucket pass streams the input in order), so the
+    // transfer overlaps that pass.  Part ends fall on staging-chunk bounds.
+    const Plan& plan = *call.plan;
+    const bool overlap = plan.shards <= 1 && plan.tile_level > 0 &&
+        plan.levels[0].cap > kWalkMaxNode && dev_bytes >= kInputParts * kStageChunk;
+    InputParts input;
+    std::vector<uint64_t> part_bytes;
+    std::mutex um;
+    std::condition_variable ucv;
+    uint32_t recorded = 0;
+    bool upload_failed = false;
+    std::thread uploader;
+    struct JoinUpload {
+        std::thread& t;
+        ~JoinUpload() {
+            if (t.joinable()) t.join();
+        }
+    } join_upload{uploader};
+    if (overlap) {
+        for (uint32_t k = 0; k < kInputParts; ++k) {
+            const uint64_t want = dev_bytes / kInputParts * (k + 1);
+            const uint64_t at = k + 1 == kInputParts ? dev_bytes
+                : std::min(dev_bytes, (want + kStageChunk - 1) / kStageChunk * kStageChunk);
+            part_bytes.push_back(at);
+            input.ends.push_back(at / device_width);
+        }
+        if (narrow || stage_in) {
+            uploader = std::thread([&] {
+                uint32_t next = 0;
+                const std::function<void(uint64_t)> on_issue = [&](uint64_t bytes) {
+                    while (next < kInputParts && bytes >= part_bytes[next]) {
+                        check(cudaEventRecord(w.inparts[next], w.copy_stream), "cudaEventRecord");
+                        {
+                            std::lock_guard<std::mutex> lock(um);
+                            recorded = ++next;
+                        }
+                        ucv.notify_all();
+                    }
+                };
+                bool ok = false;
+                try {
+                    ok = upload_staged(fill, dev_bytes, (unsigned char*)w.input, *ring->r,
+                        w.copy_stream, narrow ? narrow_threads() : 0, &on_issue);
+                } catch (const CudaFail&) {
+                    ok = false;
+                }
+                if (!ok || next < kInputParts) {
+                    std::lock_guard<std::mutex> lock(um);
+                    upload_failed = true;
+                }
+                ucv.notify_all();
+            });
+            input.wait = [&](uint32_t k) {
+                {
+                    std::unique_lock<std::mutex> lock(um);
+                    ucv.wait(lock, [&] { return upload_failed || recorded > k; });
+                    if (recorded <= k) {
+                        throw CudaFail{cudaErrorUnknown, "input upload"};
+                    }
+                }
+                check(cudaStreamWaitEvent(w.stream, w.inparts[k], 0), "cudaStreamWaitEvent");
+                if (k + 1 == kInputParts && uploader.joinable()) {
+                    uploader.join(); // every chunk is queued; the ring is free for downloads
+                }
+            };
+        } else {
+            uint64_t lo = 0;
+            for (uint32_t k = 0; k < kInputParts; ++k) {
+                check(cudaMemcpyAsync((unsigned char*)w.input + lo, src8 + lo, part_bytes[k] - lo,
+                          cudaMemcpyHostToDevice, w.copy_stream),
+                    "input upload");
+                check(cudaEventRecord(w.inparts[k], w.copy_stream), "cudaEventRecord");
+                lo = part_bytes[k];
+            }
+            input.wait = [&](uint32_t k) {
+                check(cudaStreamWaitEvent(w.stream, w.inparts[k], 0), "cudaStreamWaitEvent");
+            };
+        }
+    } else if (narrow || stage_in) {
+        upload_staged(fill, dev_bytes, (unsigned char*)w.input, *ring->r, w.stream,
+            narrow ? narrow_threads() : 0);
     } else {
         check(cudaMemcpyAsync(w.input, entries, in_bytes, cudaMemcpyHostToDevice, w.stream),
             "input upload");
+    }
+    if (!overlap && wide.load() != 0) {
+        check(cudaStreamSynchronize(w.stream), "cudaStreamSynchronize");
+        set_error(err, err_len, "input must contain every value from zero through size minus one");
+        return kInvalidArgument;
     }
     // Bytes [0, end) of the blob are the encoding; the first cluster groups
     // go down on the copy stream (through the ring on a helper thread for a
@@ -1290,7 +1409,11 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
         }
     };
     rc = run(w, call, w.stream, w.input, device_width, w.blob, device_seconds, err, err_len,
-        early.levels ? &level_hook : nullptr, early.cuts.empty() ? nullptr : &parts);
+        early.levels ? &level_hook : nullptr, early.cuts.empty() ? nullptr : &parts,
+        overlap ? &input : nullptr);
+    if (uploader.joinable()) {
+        uploader.join();
+    }
     {
         std::lock_guard<std::mutex> lock(qm);
         closed = true;
@@ -1300,6 +1423,10 @@ int compress_host(const void* entries, uint64_t count, uint32_t entry_bytes,
         helper.join();
     }
     check(cudaStreamSynchronize(w.copy_stream), "cudaStreamSynchronize");
+    if (wide.load() != 0) {
+        set_error(err, err_len, "input must contain every value from zero through size minus one");
+        return kInvalidArgument;
+    }
     if (rc != kOk) {
         return rc;
     }

@@ -184,19 +184,24 @@ constexpr int kBucketItems = 16;
 constexpr int kBucketThreads = BPB200_BUCKET_THREADS; // block size of level_bucket
 
 template <typename T>
+// Slots [e_lo, e_hi) of the level (the whole level, or one part of an input
+// still being uploaded; e_lo a multiple of 4 so vector loads stay aligned).
 __device__ __forceinline__ void level_bucket_run(Grid grid, const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
-    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
+    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status,
+    uint64_t e_lo, uint64_t e_hi) {
     __shared__ uint32_t count[kMaxWindows];
     __shared__ uint32_t start[kMaxWindows];
     const LevelInfo& lv = plan->levels[level];
     const uint32_t cap = (uint32_t)lv.cap;
     const uint32_t pcap = (uint32_t)lv.pcap;
-    const uint64_t total = (uint64_t)cap << level;
-    const uint32_t windows = (uint32_t)((total + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
+    const uint64_t slots = (uint64_t)cap << level;
+    const uint64_t total = e_hi < slots ? e_hi : slots;
+    const uint32_t windows = (uint32_t)((slots + (1ull << kPlaceLog2) - 1) >> kPlaceLog2);
     const uint64_t chunk = (uint64_t)blockDim.x * kBucketItems;
-    const bool aligned = ((uintptr_t)src & 15u) == 0;
-    for (uint64_t c0 = (uint64_t)grid.bid * chunk; c0 < total; c0 += (uint64_t)grid.nblk * chunk) {
+    const bool aligned = ((uintptr_t)src & 15u) == 0 && (e_lo & 3u) == 0;
+    for (uint64_t c0 = e_lo + (uint64_t)grid.bid * chunk; c0 < total;
+         c0 += (uint64_t)grid.nblk * chunk) {
         for (uint32_t b = threadIdx.x; b < windows; b += blockDim.x) count[b] = 0;
         __syncthreads();
         const uint64_t e0 = c0 + (uint64_t)threadIdx.x * kBucketItems;
@@ -252,7 +257,7 @@ __device__ __forceinline__ void level_bucket_run(Grid grid, const Plan* __restri
             if (dest[q] == ~0u) continue;
             const uint32_t b = dest[q] >> kPlaceLog2;
             const uint64_t at = ((uint64_t)b << kPlaceLog2) + start[b] + atomicAdd(&count[b], 1u);
-            if (at < total && at < ((uint64_t)(b + 1) << kPlaceLog2)) {
+            if (at < slots && at < ((uint64_t)(b + 1) << kPlaceLog2)) {
                 records[at] = make_uint2(dest[q], idx[q]);
             } else {
                 atomicOr(status, kErrNotPermutation); // more values than slots: a repeat
@@ -265,8 +270,9 @@ __device__ __forceinline__ void level_bucket_run(Grid grid, const Plan* __restri
 template <typename T>
 __global__ void __launch_bounds__(BPB200_BUCKET_THREADS) level_bucket(const Plan* __restrict__ plan,
     uint32_t level, const T* __restrict__ src, uint2* __restrict__ records,
-    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status) {
-    level_bucket_run<T>(launch_grid(), plan, level, src, records, cursor, uf, status);
+    uint32_t* __restrict__ cursor, uint32_t* __restrict__ uf, uint32_t* status,
+    uint64_t e_lo, uint64_t e_hi) {
+    level_bucket_run<T>(launch_grid(), plan, level, src, records, cursor, uf, status, e_lo, e_hi);
 }
 
 constexpr int kPlaceItems = 16;

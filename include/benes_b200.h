@@ -58,7 +58,9 @@ int bpb200_encoded_size(uint64_t count, const bpb200_format* format,
  * `entry_bytes` (4 or 8) bytes.  Writes exactly `blob_len` bytes (which must
  * equal bpb200_encoded_size) into `blob`, byte-identical to the reference's
  * portable encoder.  `device_seconds` (may be NULL) receives the on-device
- * time, the value the reference stores with set_last_device_seconds.
+ * time, the value the reference stores with set_last_device_seconds (for
+ * inputs of 2^25 entries and more, from the first level-0 kernel on, which
+ * starts while the input is still being uploaded).
  * Errors: INVALID_ARGUMENT "input must contain every value from zero through
  * size minus one" for a non-permutation, exactly like validate_permutation
  * (src/benes.cpp:152-173).  Parts of the blob are copied into `blob` while

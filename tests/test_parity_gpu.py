@@ -186,6 +186,14 @@ def test_host_path_early_download(gpu, oracle):
         assert bytes(got) == want, kw
         # bytes past the encoded size are left as they were
         assert bool((pinned[size:] == 0xA5).all()), kw
+        if n > (1 << 25):
+            # inputs above 2^25 entries are uploaded in parts that level 0
+            # buckets as they arrive: from pageable memory (above), and from
+            # pinned memory straight to the device
+            held = torch.empty(n, dtype=torch.int64 if w == 8 else torch.int32,
+                               pin_memory=True).numpy().view(dtype)
+            held[:] = perm
+            assert gpu.compress(held, opts) == want, kw
         if i == 2:
             assert want == oracle.compress(perm, oracle_format(kw)), kw
 

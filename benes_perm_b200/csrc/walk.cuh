@@ -68,7 +68,6 @@ namespace bpb200 {
 #define BPB200_RESOLVE_WRITEBACK 1
 #endif
 
-
 constexpr uint32_t kRulerLog2 = BPB200_RULER_LOG2; // one ruler per 2^kRulerLog2 slots
 constexpr uint32_t kWalkCap = 1u << 16;      // longest ruler walk before giving up
 #ifndef BPB200_WALK_CHUNK

@@ -219,6 +219,18 @@ def test_host_path_narrowed_upload(gpu, oracle):
         with pytest.raises(ValueError, match="every value"):
             gpu.compress(bad, opts)
     assert gpu.compress(perm, opts) == want
+    # from 2^25 entries the narrowed upload overlaps level 0: a wide value
+    # found while the encode already runs still fails the call
+    big = (1 << 25) + 7
+    perm = gpu.fill_permutation(gpu.PermutationKind.uniform, 0x4B, big, np.uint64)
+    good = gpu.compress(perm, opts)
+    assert good == gpu.compress(perm.astype(np.uint32), opts)
+    for at in (0, big // 3, big - 1):
+        bad = perm.copy()
+        bad[at] = 1 << 40
+        with pytest.raises(ValueError, match="every value"):
+            gpu.compress(bad, opts)
+    assert gpu.compress(perm, opts) == good
 
 
 def test_invalid_inputs_then_recovery(gpu, oracle):

@@ -45,6 +45,11 @@ __host__ __device__ inline uint32_t tile_smem_layout(uint32_t slots, uint32_t pa
     return o;
 }
 
+// Uniform-level fast path for node sizes in the tile (1) or size_at everywhere (0).
+#ifndef BPB200_TILE_UNIFORM
+#define BPB200_TILE_UNIFORM 1
+#endif
+
 // Tile input through one bulk asynchronous copy (1) or batched plain loads (0).
 #ifndef BPB200_TILE_BULK_LOAD
 #define BPB200_TILE_BULK_LOAD 0
@@ -209,6 +214,17 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
         // uniform per level: whether every node here exists / is internal
         const bool all_exist = level == 0 || plan.levels[level - 1].q > leaf;
         const bool all_internal = lv.q > leaf && all_exist;
+        // node sizes: every node of a level without large nodes (r = 0, all
+        // levels of a power-of-two count) has q entries
+#if BPB200_TILE_UNIFORM
+        const uint32_t q32 = (uint32_t)lv.q;
+        const bool uniform = lv.r == 0;
+        auto node_size = [&](uint32_t node) {
+            return uniform ? q32 : size_at(lv, level, node);
+        };
+#else
+        auto node_size = [&](uint32_t node) { return size_at(lv, level, node); };
+#endif
         auto internal_node = [&](uint32_t path, uint32_t s) {
             if (all_internal) return true;
             if (s <= leaf) return false;
@@ -230,7 +246,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             for (uint32_t e = tid; t == 0 && e < nodes * cap; e += blockDim.x) {
                 const uint32_t path = by_cap(e);
                 const uint32_t i = e - path * cap;
-                const uint32_t s = size_at(lv, level, first + path);
+                const uint32_t s = node_size(first + path);
                 if (i >= s || !internal_node(path, s)) {
                     continue;
                 }
@@ -255,7 +271,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             for (uint32_t idx = tid; idx < nodes * pcap; idx += blockDim.x) {
                 const uint32_t path = idx & (nodes - 1);
                 const uint32_t k = idx >> t;
-                const uint32_t s = size_at(lv, level, first + path);
+                const uint32_t s = node_size(first + path);
                 if (k >= s / 2 || !internal_node(path, s)) {
                     continue;
                 }
@@ -271,7 +287,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
             __syncthreads();
             // C: orient odd nodes so the unpaired tail gets colour 0
             for (uint32_t path = tid; path < nodes; path += blockDim.x) {
-                const uint32_t s = size_at(lv, level, first + path);
+                const uint32_t s = node_size(first + path);
                 if ((s & 1u) == 0 || !internal_node(path, s)) {
                     continue;
                 }
@@ -294,7 +310,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 if (p < ptotal) {
                     const uint32_t path = by_pcap(p);
                     const uint32_t k = p - path * pcap;
-                    const uint32_t s = size_at(lv, level, first + path);
+                    const uint32_t s = node_size(first + path);
                     if (k < s - s / 2 && internal_node(path, s)) {
                         const Found f = uf_find(uf, p, status);
                         x = f.bit ^ (uf_load(uf, f.root) & 1u);
@@ -325,7 +341,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                 if (p < ptotal) {
                     const uint32_t path = by_pcap(p);
                     const uint32_t k = p - path * pcap;
-                    const uint32_t s = size_at(lv, level, first + path);
+                    const uint32_t s = node_size(first + path);
                     const uint32_t half = s / 2;
                     if (k <= half && internal_node(path, s)) {
                         const uint32_t lb = 2 * path * ccap;
@@ -372,7 +388,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     const uint32_t slot = tid >> 1;
                     const int side = (int)(tid & 1);
                     const uint32_t node = first + w0 + slot;
-                    const uint32_t s = size_at(lv, level, node);
+                    const uint32_t s = node_size(node);
                     if (internal_node(w0 + slot, s)) {
                         desc[side * kNodeWave + slot] = node_address(plan, side, level, node);
                     }
@@ -398,7 +414,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                             const uint32_t pair0 =
                                 (packet << span_log2) + ((rem & ((1u << cshift) - 1)) << 5);
                             const uint32_t path = w0 + slot;
-                            const uint32_t s = size_at(lv, level, first + path);
+                            const uint32_t s = node_size(first + path);
                             if (pair0 >= s / 2 || !internal_node(path, s)) {
                                 continue;
                             }
@@ -472,7 +488,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                             const uint32_t slot = rem >> span_log2;
                             const uint32_t pair = (packet << span_log2) + (rem & ((1u << span_log2) - 1));
                             const uint32_t path = w0 + slot;
-                            const uint32_t s = size_at(lv, level, first + path);
+                            const uint32_t s = node_size(first + path);
                             if (pair < s / 2 && internal_node(path, s)) {
                                 const uint32_t q = path * pcap + pair;
                                 set = ((bits[q >> 5] >> (q & 31)) & 1u) != 0;
@@ -498,7 +514,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                     uint64_t v = ~0ull;
                     const bool exists = all_exist ||
                         size_at(plan.levels[level - 1], level - 1, node >> 1) > leaf;
-                    if (size_at(lv, level, node) <= leaf && exists) {
+                    if (node_size(node) <= leaf && exists) {
                         int section = 0;
                         const uint64_t bit = leaf_rank_bit(plan, level, node, &section);
                         v = plan.section_offset[section] * 8 + bit;
@@ -512,7 +528,7 @@ __device__ __forceinline__ void tile_body(const Plan* __restrict__ plan_ptr,
                         continue;
                     }
                     const uint32_t path = w0 + li;
-                    const uint32_t s = size_at(lv, level, first + path);
+                    const uint32_t s = node_size(first + path);
                     const uint32_t v = lane < s ? (uint32_t)cur[path * cap + lane] : 0u;
                     if (lane < s && v >= s) {
                         atomicOr(status, kErrNotPermutation);

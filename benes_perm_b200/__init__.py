@@ -286,9 +286,11 @@ def set_profiling(enabled: bool) -> None:
     library().bpb200_set_profiling(1 if enabled else 0)
 
 
-def set_union_find_only(enabled: bool) -> None:
-    """Test hook: colour global levels with union-find instead of orbit walks."""
-    library().bpb200_set_colouring(1 if enabled else 0)
+def set_union_find_only(enabled) -> None:
+    """Test hook: colour global levels with union-find instead of orbit walks
+    (True), or run the walks and colour their levels with the union-find
+    fallback anyway ("fallback"); False restores the default."""
+    library().bpb200_set_colouring(2 if enabled == "fallback" else (1 if enabled else 0))
 
 
 def last_profile():

@@ -563,7 +563,10 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
     const int gw = grid_for(my_buckets, kLevelThreads);
     uint32_t* ctl = w.control;
     // nodes whose arrays do not fit in L2 are coloured by union-find
-    const bool walks = lv.cap <= (1ull << tune.walk_max_log2) && g_force_union_find.load() == 0;
+    // 0: walks where they pay; 1: union-find everywhere; 2: walks, then the
+    // union-find fallback as if they had given up (test hooks)
+    const int colouring = g_force_union_find.load();
+    const bool walks = lv.cap <= (1ull << tune.walk_max_log2) && colouring != 1;
     control_reset<<<1, 32, 0, st>>>(ctl, walks ? 0u : 1u);
     rec.launches += 1;
     if (l == 0 && lv.cap > kWalkMaxNode && w.records != nullptr) {
@@ -649,11 +652,20 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
             ruler_colour<<<gw, kLevelThreads, 0, st>>>(rr.lo, rr.hi, w.super_of, sstate[0],
                 sstate[1], ctl);
         }, one_block ? 4 : 3 + 2 * (rounds + 1));
+        if (colouring == 2) {
+            level_force_fallback<<<1, 1, 0, st>>>(ctl + kCtlHard);
+            rec.launches += 1;
+        }
     }
+    // a walk level's union-find words are set up only if it falls back
+    const bool reset_uf = walks && l > 0;
     rec.launch(kKindUnion, [&] {
+        if (reset_uf) {
+            level_uf_reset<<<gp, kLevelThreads, 0, st>>>(dp, l, w.uf, ctl + kCtlHard);
+        }
         level_union<<<gu, kLevelThreads, 0, st>>>(dp, l, inv, w.uf, ctl + kCtlHard,
             ctl + kCtlClaimUnion, w.d_status);
-    });
+    }, reset_uf ? 2 : 1);
     rec.launch(kKindOrient, [&] {
         level_orient<<<gn, kLevelThreads, 0, st>>>(dp, l, inv, w.uf, ctl + kCtlHard, w.d_status);
     });
@@ -668,9 +680,11 @@ void run_level(Workspace& w, Recorder& rec, cudaStream_t st, const Plan& p, cons
         const bool global_child = child_inv != nullptr;
         // owners only matter where the orbit walks run
         const bool child_walks = global_child && p.levels[l + 1].cap <= (1ull << tune.walk_max_log2)
-            && g_force_union_find.load() == 0;
+            && colouring != 1;
+        // union-find roots only for children coloured by union-find; a walk
+        // child sets them up itself if it falls back (level_uf_reset)
         level_outputs<<<gp, kLevelThreads, 0, st>>>(dp, l, inv, w.xbits, w.ybits, child_inv,
-            child_walks ? w.owner : nullptr, global_child ? w.uf : nullptr);
+            child_walks ? w.owner : nullptr, global_child && !child_walks ? w.uf : nullptr);
     });
     // above the shard level every shard computes the level, shard 0 alone
     // writes its switches
@@ -1564,7 +1578,9 @@ int bpb200_set_tuning(const bpb200_tuning* forced) {
     return kOk;
 }
 
-void bpb200_set_colouring(int union_find_only) { g_force_union_find.store(union_find_only ? 1 : 0); }
+void bpb200_set_colouring(int union_find_only) {
+    g_force_union_find.store(union_find_only == 2 ? 2 : (union_find_only ? 1 : 0));
+}
 
 int bpb200_describe(uint64_t count, const bpb200_format* format, uint32_t* depth,
     uint32_t* tile_level) {

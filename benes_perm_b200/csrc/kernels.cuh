@@ -375,6 +375,30 @@ __global__ void __launch_bounds__(256, BPB200_UNION_MIN_BLOCKS) level_union(cons
     level_union_run(launch_grid(), plan, level, inv, uf, hard, claims, status);
 }
 
+// Walk levels: their pair-nodes start as union-find roots only when the
+// walks gave up (the `hard` flag) and the level falls back to union-find;
+// the parent's output pass does not set them up for walk levels.
+__global__ void __launch_bounds__(256) level_uf_reset(const Plan* __restrict__ plan,
+    uint32_t level, uint32_t* __restrict__ uf, const uint32_t* hard) {
+    if (*hard == 0) {
+        return;
+    }
+    const LevelInfo& lv = plan->levels[level];
+    const NodeRange nr = level_nodes(*plan, level);
+    const uint64_t lo = nr.lo * lv.pcap;
+    const uint64_t hi = lo + (lv.pcap << nr.shift);
+    for (uint64_t id = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; id < hi;
+         id += (uint64_t)gridDim.x * blockDim.x) {
+        uf[id] = (uint32_t)id << 1;
+    }
+}
+
+// Test hook: the walks of the level ran, but the level is coloured by the
+// union-find fallback anyway, as if a walk had given up.
+__global__ void level_force_fallback(uint32_t* hard) {
+    *hard = 1;
+}
+
 __device__ __forceinline__ void level_orient_run(Grid grid, const Plan* __restrict__ plan, uint32_t level,
     const uint32_t* __restrict__ inv, uint32_t* uf, const uint32_t* hard, uint32_t* status) {
     if (hard != nullptr && *hard == 0) {

@@ -237,9 +237,12 @@ int bpb200_get_tuning(uint64_t count, bpb200_tuning* out);
  * (values clamped to their ranges); NULL returns to the table. */
 int bpb200_set_tuning(const bpb200_tuning* forced);
 
-/* Test hook: nonzero makes later calls colour every global level with the
+/* Test hook: 1 makes later calls colour every global level with the
  * union-find kernels instead of the orbit walks (the path the walks fall
- * back to on contrived inputs).  Output bytes are identical either way. */
+ * back to on contrived inputs); 2 runs the walks and then colours each walk
+ * level with that fallback anyway, as if a walk had given up (single-call
+ * paths; the batched groups treat 2 as 0); 0 restores the default.  Output
+ * bytes are identical in every mode. */
 void bpb200_set_colouring(int union_find_only);
 
 /* Geometry of the encode the library would run for (count, format): the

@@ -94,9 +94,11 @@ def test_format_options(gpu, oracle):
                     assert got == oracle.compress(perm, oracle_format(kw)), (n, kw)
 
 
-@pytest.mark.parametrize("union_find_only", [False, True])
+@pytest.mark.parametrize("union_find_only", [False, True, "fallback"])
 def test_global_levels_both_colourings(gpu, oracle, union_find_only):
-    # sizes that run several global levels (nodes above 8192 entries)
+    # sizes that run several global levels (nodes above 8192 entries);
+    # "fallback": the walks run, then every walk level is coloured by the
+    # union-find fallback, whose roots that level sets up itself
     gpu.set_union_find_only(union_find_only)
     try:
         for n, kind in ((40000, 0), (65537, 1), (131072, 4), (100003, 2), (99999, 3)):

@@ -9,18 +9,25 @@ configuration the headline metric is quoted on.  A step is one full compress
 of that permutation.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                  [--shard] [--no-serving] [--workload headline|serving]
 
 ``value``: entries/s with the input already in HBM (device-resident entry
 point), timed with CUDA events on the launching stream over exactly K steps,
 max over ranks.  ``e2e``: the same metric through the host entry point,
 including the host->device copy of the input from pinned memory and the
-device->host copy of the blob.  The path does not shard: with N GPUs every
-rank compresses its own permutation (replicas, weak scaling).  After the
-timed regions every entry of the measured blob is checked in both
-directions through the device lookup verifier and the host entry point's
-blob is compared with the device one (``verified``); a failed check exits 1.
-``--impl reference`` times the reference's portable_cpu encoder (built from
-its own sources into oracle/_ref) on the host cores instead.
+device->host copy of the blob.  With N GPUs every rank compresses its own
+permutation (replicas, weak scaling); ``--shard`` instead splits one
+permutation into N subtree shards summed on rank 0 (strong scaling).  After
+the timed regions the measured blob's SHA-256 is compared with the
+reference's digest, every entry is checked in both directions through the
+device lookup verifier, and the host entry point's blob is compared with
+the device one (``verified``); a failed check exits 1.  ``serving``: the
+mixed-size request stream through the serving loop against plain
+per-request calls (capacity: median of three runs on one warmed server;
+latency under Poisson arrivals).  ``cpu_baseline`` and ``--impl reference``
+time the reference's portable_cpu encoder (built from its own sources into
+oracle/_ref) with all host threads on a bounded 2^24-entry sample of the
+same workload, with input from the oracle's generator.
 """
 from __future__ import annotations
 
